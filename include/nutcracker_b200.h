@@ -1,0 +1,134 @@
+/*
+ * nutcracker_b200.h - C-ABI of the B200 (sm_100a) variational-MPS sweep path.
+ *
+ * Level 0: drop-in replacements for the Fortran-ABI numeric kernels that the
+ * reference's C++ layer binds in sources/common/core.cpp (declared there as
+ * extern "C" with trailing underscores).  Same names, same argument order and
+ * meaning: every scalar is passed by pointer, buffers are column-major
+ * complex128 (layout-compatible with std::complex<double>), MPO indices are
+ * uint32 (from,to) pairs, 1-based, and outputs are caller-allocated HOST
+ * buffers.  Each call copies its inputs to the GPU, runs the CUDA kernels and
+ * copies the outputs back.  Unlike the reference (which calls Fortran `stop`
+ * on LAPACK errors), no entry point ever exits the process: failures are
+ * reported through the return code where the reference has one, and always
+ * through nc_last_status()/nc_last_error().
+ *
+ * Level 1: device-resident chain handle (nc_chain_*), the performance
+ * drop-in for Nutcracker::Chain (includes/nutcracker/chain.hpp:115-235):
+ * sites, environments and projectors stay in HBM across sweeps.
+ */
+#ifndef NUTCRACKER_B200_H
+#define NUTCRACKER_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct { double re, im; } nc_complex; /* == std::complex<double> */
+
+/* ---- error reporting --------------------------------------------------- */
+/* Status of the last call on this host thread (0 = success). */
+int nc_last_status(void);
+/* Message of the last failing call on this host thread ("" if none). */
+const char* nc_last_error(void);
+/* Kernels this library has launched on this host thread's context. */
+uint64_t nc_launch_count(void);
+/* Library version string. */
+const char* nc_version(void);
+/* Enqueue this thread's work on `stream` (a cudaStream_t; NULL is the
+   legacy default stream).  Returns a status code. */
+int nc_set_stream(void* stream);
+/* Go back to the library's own non-blocking stream (the initial state). */
+int nc_use_own_stream(void);
+/* Wait for this thread's stream.  Returns a status code. */
+int nc_synchronize(void);
+
+/* Device-pointer effective-Hamiltonian product y = H_eff x for one site
+   (the strategy-3 `operate_on` of core.f95:2529-2556 without projectors):
+   L (bl,bl,cl), R (br,br,cr), x and y (br,bl,d), W (d,d,nnz), idx (2,nnz)
+   1-based, all in device memory.  Scratch comes from the library's device
+   arena.  Asynchronous on this thread's stream; returns a status code. */
+int nc_heff_apply_dev(uint32_t bl, uint32_t br, uint32_t cl, uint32_t cr, uint32_t d, uint32_t nnz,
+                      const uint32_t* idx_dev, const void* W_dev, const void* L_dev,
+                      const void* R_dev, const void* x_dev, void* y_dev);
+
+/* ---- Level 0: contractions (sources/common/core.cpp:33-420) ------------- */
+
+/* core.cpp:33-45 (compute_expectation_): <psi|H|psi> at one site. */
+void compute_expectation_(const uint32_t* bl, const uint32_t* br, const uint32_t* cl,
+                          const uint32_t* cr, const uint32_t* d, const nc_complex* left_environment,
+                          const nc_complex* state_site_tensor, const uint32_t* number_of_matrices,
+                          const uint32_t* sparse_operator_indices,
+                          const nc_complex* sparse_operator_matrices,
+                          const nc_complex* right_environment, nc_complex* expectation);
+
+/* core.cpp:75-86 (compute_optimization_matrix_): dense H_eff, (br*bl*d)^2. */
+void compute_optimization_matrix_(const uint32_t* bl, const uint32_t* br, const uint32_t* cl,
+                                  const uint32_t* cr, const uint32_t* d,
+                                  const nc_complex* left_environment,
+                                  const uint32_t* number_of_matrices,
+                                  const uint32_t* sparse_operator_indices,
+                                  const nc_complex* sparse_operator_matrices,
+                                  const nc_complex* right_environment,
+                                  nc_complex* optimization_matrix);
+
+/* core.cpp:145-150 (construct_left_exp_boundary_). */
+void construct_left_exp_boundary_(const uint32_t* b, const uint32_t* c,
+                                  const nc_complex* state_boundary,
+                                  const nc_complex* operator_boundary,
+                                  nc_complex* left_expectation_boundary);
+/* core.cpp:165-170 (construct_right_exp_boundary_). */
+void construct_right_exp_boundary_(const uint32_t* b, const uint32_t* c,
+                                   const nc_complex* state_boundary,
+                                   const nc_complex* operator_boundary,
+                                   nc_complex* right_expectation_boundary);
+/* core.cpp:185-191 (contract_expectation_boundaries_). */
+void contract_expectation_boundaries_(const uint32_t* b, const uint32_t* c,
+                                      const nc_complex* left_boundary,
+                                      const nc_complex* right_boundary, nc_complex* expectation);
+
+/* core.cpp:235-247 (contract_sos_left_): new left environment (br,br,cr). */
+void contract_sos_left_(const uint32_t* bl, const uint32_t* br, const uint32_t* cl,
+                        const uint32_t* cr, const uint32_t* d, const nc_complex* left_environment,
+                        const uint32_t* number_of_matrices, const uint32_t* sparse_operator_indices,
+                        const nc_complex* sparse_operator_matrices,
+                        const nc_complex* state_site_tensor, nc_complex* new_left_environment);
+/* core.cpp:274-286 (contract_sos_right_): new right environment (bl,bl,cl). */
+void contract_sos_right_(const uint32_t* bl, const uint32_t* br, const uint32_t* cl,
+                         const uint32_t* cr, const uint32_t* d, const nc_complex* right_environment,
+                         const uint32_t* number_of_matrices, const uint32_t* sparse_operator_indices,
+                         const nc_complex* sparse_operator_matrices,
+                         const nc_complex* state_site_tensor, nc_complex* new_right_environment);
+/* core.cpp:313-322 (contract_vs_left_). */
+void contract_vs_left_(const uint32_t* b_left_old, const uint32_t* b_right_old,
+                       const uint32_t* b_left_new, const uint32_t* b_right_new, const uint32_t* d,
+                       const nc_complex* left_environment,
+                       const nc_complex* normalized_projector_site_tensor,
+                       const nc_complex* normalized_state_site_tensor,
+                       nc_complex* new_left_environment);
+/* core.cpp:347-356 (contract_vs_right_). */
+void contract_vs_right_(const uint32_t* b_left_old, const uint32_t* b_right_old,
+                        const uint32_t* b_left_new, const uint32_t* b_right_new, const uint32_t* d,
+                        const nc_complex* right_environment,
+                        const nc_complex* normalized_projector_site_tensor,
+                        const nc_complex* normalized_state_site_tensor,
+                        nc_complex* new_right_environment);
+/* core.cpp:529-538 (form_overlap_vector_). */
+void form_overlap_vector_(const uint32_t* b_left_old, const uint32_t* b_right_old,
+                          const uint32_t* b_left_new, const uint32_t* b_right_new,
+                          const uint32_t* d, const nc_complex* left_environment,
+                          const nc_complex* right_environment,
+                          const nc_complex* unnormalized_projector_site_tensor,
+                          nc_complex* overlap_vector);
+/* core.cpp:510-515 (form_overlap_site_tensor_). */
+void form_overlap_site_tensor_(const uint32_t* br, const uint32_t* bl, const uint32_t* d,
+                               const nc_complex* state_site_tensor,
+                               nc_complex* overlap_site_tensor);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NUTCRACKER_B200_H */

@@ -1,0 +1,76 @@
+// Internal (C++) interface of the CUDA path.  All pointers are device
+// pointers; every routine enqueues on ctx.stream and returns without a host
+// synchronisation unless it returns a host value.
+#pragma once
+
+#include "nc_common.cuh"
+
+namespace nc {
+
+enum Op { OP_N = 0, OP_T = 1, OP_C = 2 };
+
+struct ZGemmParams {
+    int opA, opB;
+    int M, N, K;
+    const cplx* A; long long lda, sA0, sA1;
+    const cplx* B; long long ldb, sB0, sB1;
+    cplx* C; long long ldc, sC0, sC1;
+    int nb0, batch;   // batch index b = b0 + nb0*b1; nb0 = 0: one level (b0 = b)
+    cplx alpha, beta;
+};
+
+ZGemmParams zgemm_params(int opA, int opB, int M, int N, int K, const cplx* A, long long lda,
+                         const cplx* B, long long ldb, cplx* C, long long ldc);
+void zgemm(const ZGemmParams& p, cudaStream_t s);
+void scale_strided(const ZGemmParams& p, cudaStream_t s);
+
+// One MPO site on the device: W (d,d,nnz) column-major, idx (2,nnz) 1-based.
+struct MpoSite {
+    int d = 0, cl = 0, cr = 0, nnz = 0;
+    const uint32_t* idx = nullptr;
+    const cplx* W = nullptr;
+};
+
+// ---- sparse-MPO contractions (contract.cu) ---------------------------------
+size_t heff_workspace_elems(int bl, int br, const MpoSite& op);
+// y = H_eff x for x, y of shape (br,bl,d).  ws: heff_workspace_elems complex.
+void heff_apply(Context& ctx, int bl, int br, const MpoSite& op, const cplx* L, const cplx* R,
+                const cplx* x, cplx* y, cplx* ws);
+// New left environment (br,br,cr) from L (bl,bl,cl) and psi (br,bl,d).
+void sos_left(Context& ctx, int bl, int br, const MpoSite& op, const cplx* L, const cplx* psi,
+              cplx* Lnew);
+// New right environment (bl,bl,cl) from R (br,br,cr) and psi (br,bl,d).
+void sos_right(Context& ctx, int bl, int br, const MpoSite& op, const cplx* R, const cplx* psi,
+               cplx* Rnew);
+void vs_left(Context& ctx, int blo, int bro, int bln, int brn, int d, const cplx* Lov,
+             const cplx* P, const cplx* S, cplx* out);
+void vs_right(Context& ctx, int blo, int bro, int bln, int brn, int d, const cplx* Rov,
+              const cplx* P, const cplx* S, cplx* out);
+void overlap_vector(Context& ctx, int blo, int bro, int bln, int brn, int d, const cplx* Lov,
+                    const cplx* Rov, const cplx* P, cplx* out);
+// out(l,s,r) = conj(S(r,l,s))
+void overlap_site_from_state(Context& ctx, int br, int bl, int d, const cplx* S, cplx* out);
+// sum_{i,j,k} L(j,i,k) R(i,j,k) -> *result (device)
+void contract_exp_boundaries(Context& ctx, int b, int c, const cplx* L, const cplx* R,
+                             cplx* result);
+
+// ---- vector kernels (vector.cu) --------------------------------------------
+// out = permute(in) for 3-index column-major tensors: out axis k = in axis perm[k].
+void permute3(Context& ctx, const cplx* in, int n0, int n1, int n2, const int perm[3],
+              bool conj, cplx* out);
+// result[0] = sum conj(x) y (deterministic two-pass reduction).
+void zdotc(Context& ctx, long long n, const cplx* x, const cplx* y, cplx* result);
+// result[0] = sum |x|^2 (as .x; .y = 0)
+void znrm2sq(Context& ctx, long long n, const cplx* x, cplx* result);
+void zcopy(Context& ctx, long long n, const cplx* x, cplx* y);
+void zfill(Context& ctx, long long n, cplx v, cplx* y);
+// y = a*x + y with a read from device scalar (a_dev) times host factor s
+void zaxpy_dev(Context& ctx, long long n, const cplx* a_dev, double s, const cplx* x, cplx* y);
+void zscal_host(Context& ctx, long long n, cplx a, cplx* x);
+// x *= 1/sqrt(nrm2sq_dev->x)
+void znormalize_dev(Context& ctx, long long n, const cplx* nrm2sq_dev, cplx* x);
+// Reads one device complex to the host (synchronises ctx.stream).
+cplx read_scalar(Context& ctx, const cplx* dev);
+void read_scalars(Context& ctx, const void* dev, size_t bytes, void* host);
+
+}  // namespace nc

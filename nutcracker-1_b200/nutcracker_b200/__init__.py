@@ -1,0 +1,171 @@
+"""Python host bindings for the B200 variational-MPS sweep library.
+
+The product is the C-ABI shared library ``lib/libnutcracker_b200.so``
+(declared in ``include/nutcracker_b200.h``).  This module binds it with
+ctypes and mirrors the reference's ``Nutcracker::Core`` wrappers
+(``includes/nutcracker/core.hpp:34-302``): same function names and argument
+meaning, numpy arrays with the reference's Fortran shapes in and out.
+
+There is no CPU fallback: importing this module raises if the library is
+missing, and every call raises ``NutcrackerError`` when the library reports a
+failure.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(_PKG, "lib", "libnutcracker_b200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError("nutcracker_b200: CUDA library not built (%s); run "
+                      "`python -m nutcracker_b200.build` in nutcracker-1_b200/" % LIB_PATH)
+
+lib = ct.CDLL(LIB_PATH)
+
+C128 = np.complex128
+_u32p = ct.POINTER(ct.c_uint32)
+_vp = ct.c_void_p
+
+
+class NutcrackerError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("[%d] %s" % (code, msg))
+        self.code = code
+
+
+lib.nc_last_status.restype = ct.c_int
+lib.nc_last_error.restype = ct.c_char_p
+lib.nc_launch_count.restype = ct.c_uint64
+lib.nc_version.restype = ct.c_char_p
+
+
+def _check():
+    st = lib.nc_last_status()
+    if st != 0:
+        raise NutcrackerError(st, lib.nc_last_error().decode())
+
+
+def _u(x):
+    return ct.byref(ct.c_uint32(int(x)))
+
+
+def _c(a):
+    """Column-major complex128 buffer pointer (keeps `a` alive via caller)."""
+    return a.ctypes.data_as(_vp)
+
+
+def _F(a):
+    return np.asfortranarray(np.asarray(a, dtype=C128))
+
+
+def _idx(a):
+    return np.asfortranarray(np.asarray(a, dtype=np.uint32))
+
+
+def launch_count():
+    return int(lib.nc_launch_count())
+
+
+def version():
+    return lib.nc_version().decode()
+
+
+class Core:
+    """ctypes mirror of Nutcracker::Core (core.hpp:34-302) over the GPU library."""
+
+    @staticmethod
+    def compute_expectation(bl, br, cl, cr, d, L, S, nnz, idx, W, R):
+        L, S, W, R, idx = _F(L), _F(S), _F(W), _F(R), _idx(idx)
+        out = np.zeros(1, C128)
+        lib.compute_expectation_(_u(bl), _u(br), _u(cl), _u(cr), _u(d), _c(L), _c(S), _u(nnz),
+                                 idx.ctypes.data_as(_u32p), _c(W), _c(R), _c(out))
+        _check()
+        return complex(out[0])
+
+    @staticmethod
+    def compute_optimization_matrix(bl, br, cl, cr, d, L, nnz, idx, W, R):
+        L, W, R, idx = _F(L), _F(W), _F(R), _idx(idx)
+        n = bl * br * d
+        H = np.zeros((n, n), C128, order="F")
+        lib.compute_optimization_matrix_(_u(bl), _u(br), _u(cl), _u(cr), _u(d), _c(L), _u(nnz),
+                                         idx.ctypes.data_as(_u32p), _c(W), _c(R), _c(H))
+        _check()
+        return H
+
+    @staticmethod
+    def construct_left_exp_boundary(b, c, sb, ob):
+        sb, ob = _F(sb), _F(ob)
+        out = np.zeros((b, b, c), C128, order="F")
+        lib.construct_left_exp_boundary_(_u(b), _u(c), _c(sb), _c(ob), _c(out))
+        _check()
+        return out
+
+    @staticmethod
+    def construct_right_exp_boundary(b, c, sb, ob):
+        sb, ob = _F(sb), _F(ob)
+        out = np.zeros((b, b, c), C128, order="F")
+        lib.construct_right_exp_boundary_(_u(b), _u(c), _c(sb), _c(ob), _c(out))
+        _check()
+        return out
+
+    @staticmethod
+    def contract_expectation_boundaries(b, c, L, R):
+        L, R = _F(L), _F(R)
+        out = np.zeros(1, C128)
+        lib.contract_expectation_boundaries_(_u(b), _u(c), _c(L), _c(R), _c(out))
+        _check()
+        return complex(out[0])
+
+    @staticmethod
+    def contract_sos_left(bl, br, cl, cr, d, L, nnz, idx, W, S):
+        L, W, S, idx = _F(L), _F(W), _F(S), _idx(idx)
+        out = np.zeros((br, br, cr), C128, order="F")
+        lib.contract_sos_left_(_u(bl), _u(br), _u(cl), _u(cr), _u(d), _c(L), _u(nnz),
+                               idx.ctypes.data_as(_u32p), _c(W), _c(S), _c(out))
+        _check()
+        return out
+
+    @staticmethod
+    def contract_sos_right(bl, br, cl, cr, d, R, nnz, idx, W, S):
+        R, W, S, idx = _F(R), _F(W), _F(S), _idx(idx)
+        out = np.zeros((bl, bl, cl), C128, order="F")
+        lib.contract_sos_right_(_u(bl), _u(br), _u(cl), _u(cr), _u(d), _c(R), _u(nnz),
+                                idx.ctypes.data_as(_u32p), _c(W), _c(S), _c(out))
+        _check()
+        return out
+
+    @staticmethod
+    def contract_vs_left(blo, bro, bln, brn, d, Lov, P, S):
+        Lov, P, S = _F(Lov), _F(P), _F(S)
+        out = np.zeros((brn, bro), C128, order="F")
+        lib.contract_vs_left_(_u(blo), _u(bro), _u(bln), _u(brn), _u(d), _c(Lov), _c(P), _c(S), _c(out))
+        _check()
+        return out
+
+    @staticmethod
+    def contract_vs_right(blo, bro, bln, brn, d, Rov, P, S):
+        Rov, P, S = _F(Rov), _F(P), _F(S)
+        out = np.zeros((blo, bln), C128, order="F")
+        lib.contract_vs_right_(_u(blo), _u(bro), _u(bln), _u(brn), _u(d), _c(Rov), _c(P), _c(S), _c(out))
+        _check()
+        return out
+
+    @staticmethod
+    def form_overlap_vector(blo, bro, bln, brn, d, Lov, Rov, P):
+        Lov, Rov, P = _F(Lov), _F(Rov), _F(P)
+        out = np.zeros((brn, bln, d), C128, order="F")
+        lib.form_overlap_vector_(_u(blo), _u(bro), _u(bln), _u(brn), _u(d), _c(Lov), _c(Rov), _c(P), _c(out))
+        _check()
+        return out
+
+    @staticmethod
+    def form_overlap_site_tensor(br, bl, d, S):
+        S = _F(S)
+        out = np.zeros((bl, d, br), C128, order="F")
+        lib.form_overlap_site_tensor_(_u(br), _u(bl), _u(d), _c(S), _c(out))
+        _check()
+        return out
