@@ -127,6 +127,59 @@ void form_overlap_site_tensor_(const uint32_t* br, const uint32_t* bl, const uin
                                const nc_complex* state_site_tensor,
                                nc_complex* overlap_site_tensor);
 
+/* ---- Level 0: site eigen-solve and projectors (core.cpp:420-760) -------- */
+
+/* core.cpp:676-693 (optimize_): the site eigen-solve.  Returns the
+   reference's info code: 0 success, 5 orthogonal dimension too large,
+   10 no room left by the projectors, 11 guess inside the projector space,
+   -14 (as uint32) no convergence within `number_of_iterations` restart
+   cycles; 0xFFFFFFFF on an argument/CUDA error (see nc_last_error()).
+   `which` is the 2-character ARPACK selector "SR", "LR" or "LM"; on output
+   number_of_iterations holds the number of H_eff products (0 when the
+   orthogonal space has at most 4 dimensions, like the reference's dense
+   strategy 1). */
+uint32_t optimize_(const uint32_t* bl, const uint32_t* br, const uint32_t* cl, const uint32_t* cr,
+                   const uint32_t* d, const nc_complex* left_environment,
+                   const uint32_t* number_of_matrices, const uint32_t* sparse_operator_indices,
+                   const nc_complex* sparse_operator_matrices, const nc_complex* right_environment,
+                   const uint32_t* number_of_projectors, const uint32_t* number_of_reflectors,
+                   const uint32_t* orthogonal_subspace_dimension, const nc_complex* reflectors,
+                   const nc_complex* coefficients, const uint32_t* swaps, const char* which,
+                   const double* tol, uint32_t* number_of_iterations, const nc_complex* guess,
+                   nc_complex* result, nc_complex* eigenvalue, double* normal);
+
+/* core.cpp:370-391 (convert_vectors_to_reflectors_): pivoted Householder QR
+   of `m` overlap vectors of length `n`, in place; rank and swaps out. */
+void convert_vectors_to_reflectors_(const uint32_t* n, const uint32_t* m, nc_complex* vectors,
+                                    uint32_t* rank, nc_complex* coefficients, uint32_t* swaps);
+
+/* core.cpp:425-449 (filter_components_outside_orthog_): output = the input
+   with its components in the projector space removed. */
+void filter_components_outside_orthog_(const uint32_t* full_space_dimension,
+                                       const uint32_t* number_of_projectors,
+                                       const uint32_t* number_of_reflectors,
+                                       const uint32_t* orthogonal_subspace_dimension,
+                                       const nc_complex* reflectors, const nc_complex* coefficients,
+                                       const uint32_t* swaps, const nc_complex* input,
+                                       nc_complex* output);
+
+/* core.cpp:107-134 (compute_overlap_with_projectors_): the Fortran routine
+   writes a real overlap; it is returned in overlap->re with overlap->im = 0. */
+void compute_overlap_with_projectors_(const uint32_t* number_of_projectors,
+                                      const uint32_t* number_of_reflectors,
+                                      const nc_complex* reflectors, const nc_complex* coefficients,
+                                      const uint32_t* swaps, const uint32_t* vector_size,
+                                      const nc_complex* vector, nc_complex* overlap);
+
+/* core.cpp:766-781 (random_projector_matrix_): reflectors of random
+   projector vectors (seeded device generator instead of gfortran rand()). */
+void random_projector_matrix_(const uint32_t* projector_length, const uint32_t* number_of_projectors,
+                              uint32_t* rank, nc_complex* reflectors, nc_complex* coefficients,
+                              uint32_t* swaps);
+
+/* Lanczos basis size used by optimize_ on this thread (default 24). */
+int nc_set_krylov_dimension(int m);
+
 #ifdef __cplusplus
 }
 #endif

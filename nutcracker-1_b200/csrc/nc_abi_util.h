@@ -12,6 +12,7 @@
 namespace nc {
 
 void set_status(int code, const char* msg);
+extern thread_local int g_status;
 
 // Stages host inputs into the thread's device arena and copies results back.
 struct HostStage {

@@ -96,6 +96,7 @@ struct Context {
     void* pinned = nullptr;  // small pinned host staging buffer for scalars
     size_t pinned_bytes = 0;
     uint64_t launches = 0;   // kernels launched by this library on this context
+    int krylov_dim = 24;     // Lanczos basis size before a restart
     Context();
     ~Context();
     static Context& get();   // thread-local default context

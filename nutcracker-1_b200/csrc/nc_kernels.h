@@ -72,5 +72,54 @@ void znormalize_dev(Context& ctx, long long n, const cplx* nrm2sq_dev, cplx* x);
 // Reads one device complex to the host (synchronises ctx.stream).
 cplx read_scalar(Context& ctx, const cplx* dev);
 void read_scalars(Context& ctx, const void* dev, size_t bytes, void* host);
+// Fills x with seeded uniform (-0.5,0.5] real and imaginary parts.
+void zrandom(Context& ctx, long long n, uint64_t seed, cplx* x);
+
+// ---- projector algebra (householder.cu) -------------------------------------
+constexpr int kMaxProjectors = 16;
+
+// ProjectorMatrix (includes/nutcracker/projectors.hpp:93-203) on the device.
+struct DevProjector {
+    int nproj = 0, nrefl = 0;
+    long long n = 0, orth_dim = 0;
+    const cplx* refl = nullptr;     // (n, nproj) column-major reflectors + R
+    const cplx* tau = nullptr;      // (nrefl)
+    std::vector<uint32_t> swaps;    // host copy, 1-based, size nrefl
+};
+// x <- x Q (conj_trans=false) or x Q^H for the 1 x n row vector x.
+void apply_q_row(Context& ctx, const DevProjector& P, cplx* x, bool conj_trans);
+// out = unproject(project(in)) (core.f95:1866-1909); in may equal out.
+void filter_outside(Context& ctx, const DevProjector& P, const cplx* in, cplx* out);
+// core.f95:1266-1339; synchronises.
+double overlap_with_projectors(Context& ctx, const DevProjector& P, const cplx* x);
+// Reduced-space positions removed by the filter, in order.
+std::vector<long long> removed_positions(const DevProjector& P);
+// U (n x r) orthonormal basis of the removed space (r = n - orth_dim).
+void removed_basis(Context& ctx, const DevProjector& P, cplx* U);
+// unproject_from_orthogonal_space of the reduced unit vector e_j.
+void unproject_unit(Context& ctx, const DevProjector& P, long long reduced_index, cplx* out);
+// zgeqp3 + rank rule (core.f95:1341-1435); A (m x n) overwritten with the
+// reflectors and R; returns the rank; swaps gets min(m,n) 1-based entries.
+int convert_vectors_to_reflectors_dev(Context& ctx, long long m, int n, cplx* A, cplx* tau_dev,
+                                      std::vector<uint32_t>& swaps);
+
+// ---- Krylov eigensolver (lanczos.cu) -----------------------------------------
+// w -= sum_i h_i V_i and h = V^H w helpers (V: k columns of length n, ld n).
+void multi_dotc(Context& ctx, long long n, int k, const cplx* V, const cplx* w, cplx* h);
+void multi_axpy(Context& ctx, long long n, int k, const cplx* V, const cplx* h, double sign, cplx* w);
+
+enum Which { WHICH_SR = 0, WHICH_LR = 1, WHICH_LM = 2 };
+int parse_which(const char* which);
+
+struct EigenStats {
+    int matvecs = 0;
+    int restarts = 0;
+};
+
+// The site eigen-solve of core.f95:1911-2609 on the device.  Returns the
+// reference's info code (0, 5, 10, 11, -14).
+int optimize_site(Context& ctx, int bl, int br, const MpoSite& op, const cplx* L, const cplx* R,
+                  const DevProjector& P, int which, double tol, int maxit, const cplx* guess,
+                  cplx* result, double* eigenvalue, double* normal, EigenStats* stats);
 
 }  // namespace nc

@@ -169,3 +169,88 @@ class Core:
         lib.form_overlap_site_tensor_(_u(br), _u(bl), _u(d), _c(S), _c(out))
         _check()
         return out
+
+
+def _int32(u):
+    u = int(u) & 0xFFFFFFFF
+    return u - (1 << 32) if u >= (1 << 31) else u
+
+
+class _CoreSolver:
+    @staticmethod
+    def optimize(bl, br, cl, cr, d, L, nnz, idx, W, R, nproj, nrefl, orth_dim, reflectors, coefficients,
+                 swaps, which, tol, iterations, guess):
+        """core.cpp:694-733.  Returns (info, iterations, eigenvalue, result, normal)."""
+        L, W, R, guess, idx = _F(L), _F(W), _F(R), _F(guess), _idx(idx)
+        if nproj:
+            reflectors, coefficients = _F(reflectors), _F(coefficients)
+            swaps = _idx(swaps)
+            rp, cp, sp = _c(reflectors), _c(coefficients), swaps.ctypes.data_as(_u32p)
+        else:
+            rp = cp = sp = None
+        result = np.zeros((br, bl, d), C128, order="F")
+        ev = np.zeros(1, C128)
+        normal = ct.c_double(0)
+        it = ct.c_uint32(int(iterations))
+        w = ct.create_string_buffer(which.encode() if isinstance(which, str) else which, 2)
+        lib.optimize_.restype = ct.c_uint32
+        info = lib.optimize_(_u(bl), _u(br), _u(cl), _u(cr), _u(d), _c(L), _u(nnz), idx.ctypes.data_as(_u32p),
+                             _c(W), _c(R), _u(nproj), _u(nrefl), _u(orth_dim), rp, cp, sp, w,
+                             ct.byref(ct.c_double(tol)), ct.byref(it), _c(guess), _c(result), _c(ev),
+                             ct.byref(normal))
+        _check()
+        return _int32(info), int(it.value), complex(ev[0]), result, float(normal.value)
+
+    @staticmethod
+    def convert_vectors_to_reflectors(n, m, vectors):
+        """core.cpp:370-391.  Returns (reflectors, rank, coefficients, swaps)."""
+        v = np.array(_F(vectors), order="F", copy=True)
+        k = min(n, m)
+        coeff = np.zeros(max(k, 1), C128)
+        swaps = np.zeros(max(k, 1), np.uint32)
+        rank = ct.c_uint32(0)
+        lib.convert_vectors_to_reflectors_(_u(n), _u(m), _c(v), ct.byref(rank), _c(coeff),
+                                           swaps.ctypes.data_as(_u32p))
+        _check()
+        return v, int(rank.value), coeff[:k], swaps[:k]
+
+    @staticmethod
+    def filter_components_outside_orthog(n, nproj, nrefl, orth_dim, reflectors, coefficients, swaps, x):
+        reflectors, coefficients, x, swaps = _F(reflectors), _F(coefficients), _F(x), _idx(swaps)
+        out = np.zeros(n, C128)
+        lib.filter_components_outside_orthog_(_u(n), _u(nproj), _u(nrefl), _u(orth_dim), _c(reflectors),
+                                              _c(coefficients), swaps.ctypes.data_as(_u32p), _c(x), _c(out))
+        _check()
+        return out
+
+    @staticmethod
+    def compute_overlap_with_projectors(nproj, nrefl, reflectors, coefficients, swaps, n, x):
+        reflectors, coefficients, x, swaps = _F(reflectors), _F(coefficients), _F(x), _idx(swaps)
+        out = np.zeros(1, C128)
+        lib.compute_overlap_with_projectors_(_u(nproj), _u(nrefl), _c(reflectors), _c(coefficients),
+                                             swaps.ctypes.data_as(_u32p), _u(n), _c(x), _c(out))
+        _check()
+        return complex(out[0])
+
+    @staticmethod
+    def random_projector_matrix(length, nproj):
+        """core.cpp:766-781 / projectors.cpp:145-171.  Returns (rank, reflectors, coefficients, swaps)."""
+        k = min(length, nproj)
+        refl = np.zeros((length, nproj), C128, order="F")
+        coeff = np.zeros(max(k, 1), C128)
+        swaps = np.zeros(max(k, 1), np.uint32)
+        rank = ct.c_uint32(0)
+        lib.random_projector_matrix_(_u(length), _u(nproj), ct.byref(rank), _c(refl), _c(coeff),
+                                     swaps.ctypes.data_as(_u32p))
+        _check()
+        return int(rank.value), refl, coeff[:k], swaps[:k]
+
+
+for _name in ("optimize", "convert_vectors_to_reflectors", "filter_components_outside_orthog",
+              "compute_overlap_with_projectors", "random_projector_matrix"):
+    setattr(Core, _name, getattr(_CoreSolver, _name))
+
+
+def set_krylov_dimension(m):
+    if lib.nc_set_krylov_dimension(int(m)) != 0:
+        _check()
