@@ -180,6 +180,131 @@ void random_projector_matrix_(const uint32_t* projector_length, const uint32_t* 
 /* Lanczos basis size used by optimize_ on this thread (default 24). */
 int nc_set_krylov_dimension(int m);
 
+/* ---- Level 0: gauge moves and random sites (core.cpp:580-680, 736-765) --
+   The device path uses a Householder-QR gauge (A = P Q with Q row-
+   orthonormal) instead of the reference's SVD polar factor; the normalised
+   and denormalised outputs differ from the reference element-wise by a
+   unitary on the shared bond, and every contraction of the pair (state,
+   energies, environments, overlaps) is identical.  Return 0 on success,
+   a nonzero status otherwise. */
+
+/* core.cpp:601-628 (norm_denorm_going_left_): site_tensor_to_normalize
+   (br,bm,dr) becomes right-normalised, site_tensor_to_denormalize (bm,bl,dl)
+   absorbs the factor. */
+int32_t norm_denorm_going_left_(const uint32_t* bl, const uint32_t* bm, const uint32_t* br,
+                                const uint32_t* dl, const uint32_t* dr,
+                                const nc_complex* site_tensor_to_denormalize,
+                                const nc_complex* site_tensor_to_normalize,
+                                nc_complex* denormalized_site_tensor,
+                                nc_complex* normalized_site_tensor);
+/* core.cpp:632-659 (norm_denorm_going_right_): site_tensor_to_normalize
+   (bm,bl,dl) becomes left-normalised, site_tensor_to_denormalize (br,bm,dr)
+   absorbs the factor. */
+int32_t norm_denorm_going_right_(const uint32_t* bl, const uint32_t* bm, const uint32_t* br,
+                                 const uint32_t* dl, const uint32_t* dr,
+                                 const nc_complex* site_tensor_to_normalize,
+                                 const nc_complex* site_tensor_to_denormalize,
+                                 nc_complex* normalized_site_tensor,
+                                 nc_complex* denormalized_site_tensor);
+/* core.cpp:663-677 (norm_for_left_): left-normalised factor of a site. */
+int32_t norm_for_left_(const uint32_t* br, const uint32_t* bl, const uint32_t* d,
+                       const nc_complex* site_tensor, nc_complex* normalized_site_tensor);
+/* core.cpp:681-695 (norm_for_right_): right-normalised factor of a site. */
+int32_t norm_for_right_(const uint32_t* br, const uint32_t* bl, const uint32_t* d,
+                        const nc_complex* site_tensor, nc_complex* normalized_site_tensor);
+/* core.cpp:570-599 (increase_bandwidth_between_): grow the bond between a
+   normalised site (bm,bl,dl) and its right neighbour (br,bm,dr) to new_bm;
+   outputs (new_bm,bl,dl) carrying the weight and (br,new_bm,dr) right-
+   normalised. */
+int32_t increase_bandwidth_between_(const uint32_t* bl, const uint32_t* bm, const uint32_t* br,
+                                    const uint32_t* dl, const uint32_t* dr, const uint32_t* new_bm,
+                                    const nc_complex* site_tensor_to_normalize,
+                                    const nc_complex* site_tensor_to_denormalize,
+                                    nc_complex* normalized_site_tensor,
+                                    nc_complex* denormalized_site_tensor);
+/* core.cpp:736-747 (rand_norm_state_site_tensor_): right-normalised random
+   site (seeded device generator). */
+void rand_norm_state_site_tensor_(const uint32_t* br, const uint32_t* bl, const uint32_t* d,
+                                  nc_complex* state_site_tensor);
+/* core.cpp:751-762 (rand_unnorm_state_site_tensor_): random site of unit norm. */
+void rand_unnorm_state_site_tensor_(const uint32_t* br, const uint32_t* bl, const uint32_t* d,
+                                    nc_complex* state_site_tensor);
+/* core.cpp:463-489 (form_norm_overlap_tensors_): the projector sites of one
+   bond (left-normalised and centre overlap sites of site 1, site 2 with the
+   factor absorbed, right-normalised overlap site of site 2). */
+void form_norm_overlap_tensors_(const uint32_t* bl, const uint32_t* bm, const uint32_t* br,
+                                const uint32_t* dl, const uint32_t* dr,
+                                const nc_complex* unnormalized_state_tensor_1,
+                                const nc_complex* right_norm_state_tensor_2,
+                                nc_complex* left_norm_overlap_tensor_1,
+                                nc_complex* unnormalized_overlap_tensor_1,
+                                nc_complex* unnormalized_state_tensor_2,
+                                nc_complex* right_norm_overlap_tensor_2);
+
+/* ---- Level 1: device-resident chain (chain.hpp:115-235) ---------------- */
+
+/* ChainOptions (chain_options.hpp:11-48); nc_chain_options_init fills the
+   reference defaults of chain_options.cpp:21-30. */
+typedef struct {
+    uint32_t maximum_number_of_iterations;
+    double sanity_check_threshold;
+    double site_convergence_threshold;
+    double sweep_convergence_threshold;
+    double chain_convergence_threshold;
+    uint32_t initial_bandwidth_dimension;
+    uint32_t bandwidth_increment;     /* new bandwidth = old + increment */
+    char optimizer_mode[4];           /* "<v", ">v" or ">m" */
+    uint32_t krylov_dimension;        /* Lanczos basis size (default 24) */
+    uint64_t seed;                    /* random initial states */
+    uint32_t strict;                  /* nonzero: a failed site solve is an error */
+} nc_chain_options;
+
+/* One MPO site (OperatorSite, tensors.hpp:1641-1854): indices (2,nnz)
+   1-based (from,to); matrices (d,d,nnz) column-major, host memory. */
+typedef struct {
+    uint32_t physical_dimension, left_dimension, right_dimension, number_of_matrices;
+    const uint32_t* indices;
+    const nc_complex* matrices;
+} nc_operator_site;
+
+typedef struct {
+    uint32_t number_of_sites, current_site, bandwidth_dimension, maximum_bandwidth_dimension;
+    uint32_t number_of_projectors;
+    uint64_t sweeps, site_solves, matvecs, moves, failures;
+    int32_t last_failure;             /* optimizer failure kind, 0 = none */
+    double energy;
+} nc_chain_info;
+
+typedef struct nc_chain nc_chain;
+
+void nc_chain_options_init(nc_chain_options* options);
+/* Chain(Operator, ChainOptions): copies the operator to the GPU and resets
+   to a random state (chain.cpp:37-48).  NULL on error (see nc_last_error). */
+nc_chain* nc_chain_create(uint32_t number_of_sites, const nc_operator_site* sites,
+                          const nc_chain_options* options);
+void nc_chain_free(nc_chain* chain);
+/* chain.cpp:175-237 */
+int nc_chain_reset(nc_chain* chain);
+/* Reset from an explicit state: bond dimensions (N+1 entries, both ends 1)
+   and host site tensors (br,bl,d), site 0 the centre, the rest right-
+   normalised. */
+int nc_chain_set_state(nc_chain* chain, const uint32_t* bond_dimensions,
+                       const nc_complex* const* sites);
+int nc_chain_optimize_site(nc_chain* chain);                 /* base_chain.cpp:81-110 */
+int nc_chain_perform_optimization_sweep(nc_chain* chain);    /* chain.cpp:147-163 */
+int nc_chain_sweep_until_converged(nc_chain* chain);         /* base_chain.cpp:112-123 */
+int nc_chain_optimize_chain(nc_chain* chain);                /* base_chain.cpp:64-79 */
+int nc_chain_increase_bandwidth_dimension(nc_chain* chain, uint32_t new_dimension); /* chain.cpp:75-122 */
+int nc_chain_construct_and_add_projector_from_state(nc_chain* chain);  /* chain.cpp:63-73 */
+/* solveForEigenvalues (chain.cpp:292-310): `eigenvalues` receives n levels. */
+int nc_chain_solve_for_eigenvalues(nc_chain* chain, uint32_t number_of_levels, double* eigenvalues);
+int nc_chain_move_to(nc_chain* chain, uint32_t site);        /* chain.cpp:124-133 */
+int nc_chain_get_energy(nc_chain* chain, double* energy);
+int nc_chain_compute_expectation_value(nc_chain* chain, double* value);
+int nc_chain_get_info(nc_chain* chain, nc_chain_info* info);
+/* Copies site i to host `out` (may be NULL) and writes dims (br,bl,d). */
+int nc_chain_get_site(nc_chain* chain, uint32_t i, nc_complex* out, uint32_t* dims);
+
 #ifdef __cplusplus
 }
 #endif

@@ -126,8 +126,7 @@ void stage_a(Context& ctx, int bl, int br, const MpoSite& op, const cplx* L, con
     ZGemmParams p = zgemm_params(OP_N, OP_N, br, bl * op.cl, bl, psi, br, L, bl, T, br);
     p.batch = op.d;
     p.sA0 = (long long)br * bl; p.sB0 = 0; p.sC0 = (long long)br * bl * op.cl;
-    zgemm(p, ctx.stream);
-    ctx.launches++;
+    zgemm(p, ctx);
 }
 
 }  // namespace
@@ -147,8 +146,7 @@ void heff_apply(Context& ctx, int bl, int br, const MpoSite& op, const cplx* L, 
     ZGemmParams p = zgemm_params(OP_N, OP_N, br, bl, br * op.cr, R, br, U, (long long)br * op.cr, y, br);
     p.batch = op.d;
     p.sA0 = 0; p.sB0 = (long long)br * op.cr * bl; p.sC0 = (long long)br * bl;
-    zgemm(p, ctx.stream);
-    ctx.launches++;
+    zgemm(p, ctx);
 }
 
 void sos_left(Context& ctx, int bl, int br, const MpoSite& op, const cplx* L, const cplx* psi,
@@ -164,8 +162,7 @@ void sos_left(Context& ctx, int bl, int br, const MpoSite& op, const cplx* L, co
     ZGemmParams p = zgemm_params(OP_N, OP_C, br, br, bl * op.d, U, (long long)br * op.cr, psi, br, Lnew, br);
     p.batch = op.cr;
     p.sA0 = br; p.sB0 = 0; p.sC0 = (long long)br * br;
-    zgemm(p, ctx.stream);
-    ctx.launches++;
+    zgemm(p, ctx);
 }
 
 void sos_right(Context& ctx, int bl, int br, const MpoSite& op, const cplx* R, const cplx* psi,
@@ -178,8 +175,7 @@ void sos_right(Context& ctx, int bl, int br, const MpoSite& op, const cplx* R, c
     cplx* Pp = ctx.arena.alloc_n<cplx>((size_t)br * d * bl);
     // Y(x,b,r,k2) = sum_r'' conj(psi(r'',x,b)) R(r'',r,k2)
     ZGemmParams p = zgemm_params(OP_C, OP_N, bl * d, br * op.cr, br, psi, br, R, br, Y, (long long)bl * d);
-    zgemm(p, ctx.stream);
-    ctx.launches++;
+    zgemm(p, ctx);
     long long total = (long long)bl * br * d * op.cl;
     mix_right_kernel<<<grid_for(total, 256), 256, 0, ctx.stream>>>(br, bl, op.cl, op.cr, d, op.nnz,
                                                                     op.idx, op.W, Y, Z);
@@ -192,8 +188,7 @@ void sos_right(Context& ctx, int bl, int br, const MpoSite& op, const cplx* R, c
     ZGemmParams q = zgemm_params(OP_N, OP_N, bl, bl, br * d, Z, bl, Pp, (long long)br * d, Rnew, bl);
     q.batch = op.cl;
     q.sA0 = (long long)bl * br * d; q.sB0 = 0; q.sC0 = (long long)bl * bl;
-    zgemm(q, ctx.stream);
-    ctx.launches++;
+    zgemm(q, ctx);
 }
 
 void vs_left(Context& ctx, int blo, int bro, int bln, int brn, int d, const cplx* Lov,
@@ -201,9 +196,8 @@ void vs_left(Context& ctx, int blo, int bro, int bln, int brn, int d, const cplx
     // core.f95:850-896
     ArenaFrame f(ctx.arena);
     cplx* I = ctx.arena.alloc_n<cplx>((size_t)bln * d * bro);
-    zgemm(zgemm_params(OP_N, OP_N, bln, d * bro, blo, Lov, bln, P, blo, I, bln), ctx.stream);
-    zgemm(zgemm_params(OP_N, OP_N, brn, bro, bln * d, S, brn, I, (long long)bln * d, out, brn), ctx.stream);
-    ctx.launches += 2;
+    zgemm(zgemm_params(OP_N, OP_N, bln, d * bro, blo, Lov, bln, P, blo, I, bln), ctx);
+    zgemm(zgemm_params(OP_N, OP_N, brn, bro, bln * d, S, brn, I, (long long)bln * d, out, brn), ctx);
 }
 
 void vs_right(Context& ctx, int blo, int bro, int bln, int brn, int d, const cplx* Rov,
@@ -213,11 +207,10 @@ void vs_right(Context& ctx, int blo, int bro, int bln, int brn, int d, const cpl
     cplx* I = ctx.arena.alloc_n<cplx>((size_t)blo * d * brn);
     cplx* Ts = ctx.arena.alloc_n<cplx>((size_t)d * brn * bln);
     zgemm(zgemm_params(OP_N, OP_N, blo * d, brn, bro, P, (long long)blo * d, Rov, bro, I, (long long)blo * d),
-          ctx.stream);
+          ctx);
     const int perm[3] = {2, 0, 1};  // Ts(s,r,l) = S(r,l,s)
     permute3(ctx, S, brn, bln, d, perm, false, Ts);
-    zgemm(zgemm_params(OP_N, OP_N, blo, bln, d * brn, I, blo, Ts, (long long)d * brn, out, blo), ctx.stream);
-    ctx.launches += 2;
+    zgemm(zgemm_params(OP_N, OP_N, blo, bln, d * brn, I, blo, Ts, (long long)d * brn, out, blo), ctx);
 }
 
 void overlap_vector(Context& ctx, int blo, int bro, int bln, int brn, int d, const cplx* Lov,
@@ -227,9 +220,8 @@ void overlap_vector(Context& ctx, int blo, int bro, int bln, int brn, int d, con
     cplx* I = ctx.arena.alloc_n<cplx>((size_t)blo * d * brn);
     cplx* T = ctx.arena.alloc_n<cplx>((size_t)bln * d * brn);
     zgemm(zgemm_params(OP_N, OP_N, blo * d, brn, bro, P, (long long)blo * d, Rov, bro, I, (long long)blo * d),
-          ctx.stream);
-    zgemm(zgemm_params(OP_N, OP_N, bln, d * brn, blo, Lov, bln, I, blo, T, bln), ctx.stream);
-    ctx.launches += 2;
+          ctx);
+    zgemm(zgemm_params(OP_N, OP_N, bln, d * brn, blo, Lov, bln, I, blo, T, bln), ctx);
     const int perm[3] = {2, 0, 1};  // out(r,l,s) = T(l,s,r)
     permute3(ctx, T, bln, d, brn, perm, false, out);
 }

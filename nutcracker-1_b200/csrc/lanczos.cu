@@ -30,7 +30,7 @@ namespace {
 constexpr int RT = 256;
 constexpr int RB = 296;       // 2 x 148 SMs
 constexpr int KC = 8;         // vectors per multi-dot chunk
-constexpr int MAXM = 128;     // largest Krylov basis
+constexpr int MAXM = 128;     // largest multi-dot / multi-axpy width
 
 __global__ void multi_dot_partial(long long n, int k, const cplx* __restrict__ V,
                                   const cplx* __restrict__ w, cplx* __restrict__ part) {
@@ -119,160 +119,137 @@ __global__ void random_kernel(long long n, uint64_t seed, cplx* __restrict__ x) 
     }
 }
 
-// Sturm count: number of eigenvalues of the symmetric tridiagonal (a, b) below x.
-__device__ int sturm_count(int m, const double* a, const double* b2, double x, double pivmin) {
-    int c = 0;
-    double q = a[0] - x;
-    if (fabs(q) <= pivmin) q = -pivmin;
-    if (q < 0) ++c;
-    for (int i = 1; i < m; ++i) {
-        q = a[i] - x - b2[i - 1] / q;
-        if (fabs(q) <= pivmin) q = -pivmin;
-        if (q < 0) ++c;
-    }
-    return c;
-}
+// ---- projected (Rayleigh-Ritz) problem ---------------------------------------
+// T = V^H H V is assembled column by column from the Gram-Schmidt
+// coefficients (real symmetric; a tridiagonal block plus, after a thick
+// restart, an arrow of couplings to the kept Ritz vectors).  One warp
+// diagonalises it by cyclic Jacobi with the round-robin (circle) pairing,
+// which keeps clustered Ritz values (near-degenerate doublets) orthogonal.
+constexpr int MAXT = 32;   // largest projected problem
 
-// k-th smallest eigenvalue (0-based) by 33-way multisection in one warp.
-__device__ double kth_eigenvalue(int m, const double* a, const double* b2, int k, double lo, double hi,
-                                 double pivmin) {
-    const int lane = threadIdx.x & 31;
-    for (int it = 0; it < 64; ++it) {
-        double width = hi - lo;
-        if (width <= 2.2e-16 * (fabs(lo) + fabs(hi)) + pivmin) break;
-        double x = lo + width * (double)(lane + 1) / 33.0;
-        int c = sturm_count(m, a, b2, x, pivmin);
-        unsigned mask = __ballot_sync(0xffffffffu, c >= k + 1);
-        int f = mask ? (__ffs(mask) - 1) : 32;
-        double xf = __shfl_sync(0xffffffffu, x, f < 32 ? f : 0);
-        double xl = __shfl_sync(0xffffffffu, x, f > 0 ? f - 1 : 0);
-        double nhi = (f < 32) ? xf : hi;
-        double nlo = (f > 0) ? xl : lo;
-        if (nhi == hi && nlo == lo) break;
-        hi = nhi;
-        lo = nlo;
-    }
-    return 0.5 * (lo + hi);
-}
-
-// Inverse iteration for the eigenvector of T at theta (dgttrf/dgtts2-style
-// elimination with partial pivoting; zero pivots replaced by eps*||T||).
-__device__ void tridiag_eigvec(int m, const double* a, const double* b, double theta, double tnorm,
-                               double* s) {
-    double dl[MAXM], dd[MAXM], du[MAXM], du2[MAXM];
-    int piv[MAXM];
-    const double tiny = 2.2e-16 * (tnorm > 0 ? tnorm : 1.0);
-    for (int i = 0; i < m; ++i) {
-        dd[i] = a[i] - theta;
-        if (i < m - 1) { dl[i] = b[i]; du[i] = b[i]; }
-        du2[i] = 0;
-        piv[i] = i;
-    }
-    for (int i = 0; i < m - 1; ++i) {
-        if (fabs(dd[i]) >= fabs(dl[i])) {
-            if (dd[i] == 0) dd[i] = tiny;
-            double f = dl[i] / dd[i];
-            dl[i] = f;
-            dd[i + 1] -= f * du[i];
-            du2[i] = 0;
-        } else {
-            double f = dd[i] / dl[i];
-            dd[i] = dl[i];
-            dl[i] = f;
-            double t = du[i];
-            du[i] = dd[i + 1];
-            dd[i + 1] = t - f * dd[i + 1];
-            if (i < m - 2) {
-                du2[i] = du[i + 1];
-                du[i + 1] = -f * du[i + 1];
-            }
-            piv[i] = i + 1;
-        }
-    }
-    if (dd[m - 1] == 0) dd[m - 1] = tiny;
-    for (int i = 0; i < m; ++i) s[i] = 1.0 / sqrt((double)m) * (1.0 + 0.01 * (i % 7));
-    for (int it = 0; it < 3; ++it) {
-        // forward: L
-        for (int i = 0; i < m - 1; ++i) {
-            if (piv[i] == i) {
-                s[i + 1] -= dl[i] * s[i];
-            } else {
-                double t = s[i];
-                s[i] = s[i + 1];
-                s[i + 1] = t - dl[i] * s[i];
-            }
-        }
-        // backward: U
-        s[m - 1] /= dd[m - 1];
-        if (m > 1) s[m - 2] = (s[m - 2] - du[m - 2] * s[m - 1]) / dd[m - 2];
-        for (int i = m - 3; i >= 0; --i) s[i] = (s[i] - du[i] * s[i + 1] - du2[i] * s[i + 2]) / dd[i];
-        double nr = 0;
-        for (int i = 0; i < m; ++i) nr += s[i] * s[i];
-        nr = sqrt(nr);
-        for (int i = 0; i < m; ++i) s[i] /= nr;
-    }
-    // fix the sign for determinism: largest-magnitude component positive
-    int imax = 0;
-    for (int i = 1; i < m; ++i) if (fabs(s[i]) > fabs(s[imax])) imax = i;
-    if (s[imax] < 0) for (int i = 0; i < m; ++i) s[i] = -s[i];
-}
-
-struct TriOut {
-    double theta, s_last, beta, tnorm;
+struct RitzOut {
+    double theta, res, beta, tnorm;
 };
 
-// One warp: finalise alpha_j, beta_j from the CGS coefficients, solve the
-// (j+1)-dimensional tridiagonal problem for the wanted Ritz pair.
-__global__ void lanczos_tridiag(int j, double* alpha, double* beta, const cplx* __restrict__ h1,
-                                const cplx* __restrict__ h2, const cplx* __restrict__ nrm2,
-                                int which, TriOut* out, cplx* __restrict__ s_out) {
-    __shared__ double a[MAXM], b[MAXM], b2[MAXM];
-    const int lane = threadIdx.x;
-    if (lane == 0) {
-        alpha[j] = h1[j].x + h2[j].x;
-        beta[j] = sqrt(nrm2[0].x);
-    }
-    __syncwarp();
-    const int m = j + 1;
-    for (int i = lane; i < m; i += 32) {
-        a[i] = alpha[i];
-        b[i] = (i < m - 1) ? beta[i] : 0.0;
-        b2[i] = b[i] * b[i];
-    }
-    __syncwarp();
-    double lo = 1e300, hi = -1e300, tn = 0;
-    for (int i = 0; i < m; ++i) {
-        double r = (i > 0 ? fabs(b[i - 1]) : 0) + (i < m - 1 ? fabs(b[i]) : 0);
-        lo = fmin(lo, a[i] - r);
-        hi = fmax(hi, a[i] + r);
-        tn = fmax(tn, fabs(a[i]) + r);
-    }
-    double pad = 2.2e-16 * tn * 4 + 1e-300;
-    lo -= pad;
-    hi += pad;
-    double pivmin = 1e-300 + 2.2e-16 * 2.2e-16 * tn * tn;
-    double th;
-    if (which == WHICH_SR) {
-        th = kth_eigenvalue(m, a, b2, 0, lo, hi, pivmin);
-    } else if (which == WHICH_LR) {
-        th = kth_eigenvalue(m, a, b2, m - 1, lo, hi, pivmin);
-    } else {
-        double t0 = kth_eigenvalue(m, a, b2, 0, lo, hi, pivmin);
-        double t1 = kth_eigenvalue(m, a, b2, m - 1, lo, hi, pivmin);
-        th = (fabs(t1) > fabs(t0)) ? t1 : t0;  // core.f95:446-456 picks the larger magnitude
-    }
-    if (lane == 0) {
-        double s[MAXM];
-        tridiag_eigvec(m, a, b, th, tn, s);
-        for (int i = 0; i < m; ++i) s_out[i] = cmake(s[i], 0);
-        out->theta = th;
-        out->s_last = s[m - 1];
-        out->beta = beta[j];
-        out->tnorm = tn;
+// T(i,j) = T(j,i) = Re(h1_i + h2_i), i <= j
+__global__ void fill_t_kernel(int j, const cplx* __restrict__ h1, const cplx* __restrict__ h2,
+                              double* __restrict__ T) {
+    for (int i = threadIdx.x; i <= j; i += blockDim.x) {
+        double v = h1[i].x + h2[i].x;
+        T[i + MAXT * j] = v;
+        T[j + MAXT * i] = v;
     }
 }
 
-__global__ void set_beta_zero(double* beta, int j) { beta[j] = 0.0; }
+// after a thick restart: T = diag(theta_0 .. theta_{k-1}), zero elsewhere
+__global__ void restart_t_kernel(int k, const double* __restrict__ theta, double* __restrict__ T) {
+    for (int e = threadIdx.x; e < MAXT * MAXT; e += blockDim.x) {
+        int r = e % MAXT, c = e / MAXT;
+        T[e] = (r == c && r < k) ? theta[r] : 0.0;
+    }
+}
+
+// Eigen-decomposition of the leading m x m block of T (one warp, m <= 32).
+// Ritz values are ordered by `which` (SR ascending, LR descending, LM by
+// decreasing magnitude) into theta[], vectors into S (m x m complex,
+// column-major); out gets the wanted pair's value and Ritz estimate
+// beta_j |s_{m-1,0}| (beta_j = sqrt(nrm2)).
+__global__ void ritz_kernel(int m, const double* __restrict__ T, const cplx* __restrict__ nrm2, int which,
+                            RitzOut* __restrict__ out, cplx* __restrict__ S, double* __restrict__ theta) {
+    __shared__ double A[MAXT][MAXT + 1], Vv[MAXT][MAXT + 1];
+    __shared__ double cs[MAXT / 2], sn[MAXT / 2];
+    __shared__ int pa[MAXT / 2], pb[MAXT / 2];
+    __shared__ int perm[MAXT];
+    const int lane = threadIdx.x;
+    const int mp = m + (m & 1);
+    for (int c = 0; c < mp; ++c) {
+        double v = 0.0;
+        if (lane < m && c < m) v = 0.5 * (T[lane + MAXT * c] + T[c + MAXT * lane]);
+        if (lane < mp) {
+            A[lane][c] = v;
+            Vv[lane][c] = (lane == c) ? 1.0 : 0.0;
+        }
+    }
+    __syncwarp();
+    for (int sweep = 0; sweep < 40; ++sweep) {
+        double off = 0, dg = 0;
+        if (lane < m) {
+            dg = A[lane][lane] * A[lane][lane];
+            for (int q = lane + 1; q < m; ++q) off += A[lane][q] * A[lane][q];
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            off += __shfl_xor_sync(0xffffffffu, off, o);
+            dg += __shfl_xor_sync(0xffffffffu, dg, o);
+        }
+        if (off <= 1e-32 * dg || off == 0.0) break;
+        for (int s = 0; s < mp - 1; ++s) {
+            if (lane < mp / 2) {
+                int a, b;
+                if (lane == 0) { a = mp - 1; b = s % (mp - 1); }
+                else { a = (s + lane) % (mp - 1); b = (s - lane + mp - 1) % (mp - 1); }
+                double apq = A[a][b], c = 1.0, sv = 0.0;
+                if (fabs(apq) > 1e-300) {
+                    double tau = (A[b][b] - A[a][a]) / (2.0 * apq);
+                    double t = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+                    c = 1.0 / sqrt(1.0 + t * t);
+                    sv = t * c;
+                }
+                pa[lane] = a; pb[lane] = b; cs[lane] = c; sn[lane] = sv;
+            }
+            __syncwarp();
+            if (lane < mp) {
+                for (int r = 0; r < mp / 2; ++r) {   // rows a, b of A
+                    int a = pa[r], b = pb[r];
+                    double c = cs[r], sv = sn[r];
+                    double xa = A[a][lane], xb = A[b][lane];
+                    A[a][lane] = c * xa - sv * xb;
+                    A[b][lane] = sv * xa + c * xb;
+                }
+            }
+            __syncwarp();
+            if (lane < mp) {
+                for (int r = 0; r < mp / 2; ++r) {   // columns a, b of A and V
+                    int a = pa[r], b = pb[r];
+                    double c = cs[r], sv = sn[r];
+                    double xa = A[lane][a], xb = A[lane][b];
+                    A[lane][a] = c * xa - sv * xb;
+                    A[lane][b] = sv * xa + c * xb;
+                    double va = Vv[lane][a], vb = Vv[lane][b];
+                    Vv[lane][a] = c * va - sv * vb;
+                    Vv[lane][b] = sv * va + c * vb;
+                }
+            }
+            __syncwarp();
+        }
+    }
+    if (lane == 0) {
+        // order the m genuine Ritz values (a padding direction, if any, is index m)
+        for (int i = 0; i < m; ++i) perm[i] = i;
+        for (int i = 0; i < m; ++i) {
+            int best = i;
+            for (int q = i + 1; q < m; ++q) {
+                double x = A[perm[q]][perm[q]], y = A[perm[best]][perm[best]];
+                bool better = (which == WHICH_SR) ? (x < y) : (which == WHICH_LR) ? (x > y) : (fabs(x) > fabs(y));
+                if (better) best = q;
+            }
+            int t = perm[i]; perm[i] = perm[best]; perm[best] = t;
+        }
+        double tn = 0;
+        for (int i = 0; i < m; ++i) tn = fmax(tn, fabs(A[i][i]));
+        double beta = sqrt(nrm2[0].x);
+        out->theta = A[perm[0]][perm[0]];
+        out->res = beta * fabs(Vv[m - 1][perm[0]]);
+        out->beta = beta;
+        out->tnorm = tn;
+    }
+    __syncwarp();
+    for (int r = 0; r < m; ++r) {
+        int p = perm[r];
+        if (lane < m) S[lane + m * r] = cmake(Vv[lane][p], 0.0);
+        if (lane == 0) theta[r] = A[p][p];
+    }
+}
+
 
 __global__ void scale_by_inv_sqrt(long long n, const cplx* __restrict__ nrm2, const cplx* __restrict__ in,
                                   cplx* __restrict__ out) {
@@ -450,107 +427,111 @@ int optimize_site(Context& ctx, int bl, int br, const MpoSite& op, const cplx* L
         return 0;
     }
 
-    const int m_max = (int)std::min<long long>(std::min(MAXM, ctx.krylov_dim), orth_dim);
+    // ---- thick-restart Lanczos (Wu & Simon 2000) with full reorthogonalisation
+    const int m_max = (int)std::min<long long>(std::min(MAXT, ctx.krylov_dim), orth_dim);
+    const int keep = std::max(1, std::min(std::max(4, m_max / 3), m_max - 2));
     cplx* V = ctx.arena.alloc_n<cplx>((size_t)(m_max + 1) * n);
     cplx* w = ctx.arena.alloc_n<cplx>(n);
+    cplx* Y = ctx.arena.alloc_n<cplx>((size_t)keep * n);
     cplx* h1 = ctx.arena.alloc_n<cplx>(m_max + 1);
     cplx* h2 = ctx.arena.alloc_n<cplx>(m_max + 1);
     cplx* nr = ctx.arena.alloc_n<cplx>(1);
-    double* alpha = ctx.arena.alloc_n<double>(m_max + 1);
-    double* beta = ctx.arena.alloc_n<double>(m_max + 1);
-    cplx* s = ctx.arena.alloc_n<cplx>(m_max + 1);
-    TriOut* tri = ctx.arena.alloc_n<TriOut>(1);
+    double* T = ctx.arena.alloc_n<double>(MAXT * MAXT);
+    double* theta = ctx.arena.alloc_n<double>(MAXT);
+    cplx* S = ctx.arena.alloc_n<cplx>(MAXT * MAXT);
+    RitzOut* ro = ctx.arena.alloc_n<RitzOut>(1);
 
     const double eps = 2.220446049250313e-16;
     const double tol_eff = std::max(tol, eps);
     const double eps23 = std::pow(eps, 2.0 / 3.0);
     uint64_t seed = 0x5EEDull + (uint64_t)n * 7919ull;
 
-    // starting vector: the projected guess (core.f95:2454), or random if it vanishes
-    auto start_vector = [&](cplx* v, const cplx* src) {
-        if (src) zcopy(ctx, n, src, v);
-        else zrandom(ctx, n, seed++, v);
+    auto orthogonalise = [&](cplx* v, int k) {  // CGS2 of v against V_0..V_{k-1}, then P filter
+        multi_dotc(ctx, n, k, V, v, h1);
+        multi_axpy(ctx, n, k, V, h1, -1.0, v);
+        multi_dotc(ctx, n, k, V, v, h2);
+        multi_axpy(ctx, n, k, V, h2, -1.0, v);
         filt.apply(ctx, n, v);
         znrm2sq(ctx, n, v, nr);
-        return read_scalar(ctx, nr).x;
     };
-    double g2 = start_vector(V, guess);
-    if (!(g2 > 1e-280)) g2 = start_vector(V, nullptr);
+    // starting vector: the projected guess (core.f95:2454), or random if it vanishes
+    zcopy(ctx, n, guess, V);
+    filt.apply(ctx, n, V);
+    znrm2sq(ctx, n, V, nr);
+    if (!(read_scalar(ctx, nr).x > 1e-280)) {
+        zrandom(ctx, n, seed++, V);
+        filt.apply(ctx, n, V);
+        znrm2sq(ctx, n, V, nr);
+    }
     scale_by_inv_sqrt<<<g1(n), 256, 0, ctx.stream>>>(n, nr, V, V);
     NC_CHECK_LAUNCH();
-    ctx.launches++;
+    restart_t_kernel<<<1, 256, 0, ctx.stream>>>(0, theta, T);
+    NC_CHECK_LAUNCH();
+    ctx.launches += 2;
 
     int restarts = 0;
+    int j = 0;
     for (;;) {
-        int jlast = -1;
-        bool converged = false;
-        TriOut T{};
-        for (int j = 0; j < m_max; ++j) {
-            cplx* vj = V + (size_t)j * n;
-            heff_apply(ctx, bl, br, op, L, R, vj, w, ws);
-            filt.apply(ctx, n, w);
-            ++st.matvecs;
-            // twice-iterated classical Gram-Schmidt against V_0..V_j
-            multi_dotc(ctx, n, j + 1, V, w, h1);
-            multi_axpy(ctx, n, j + 1, V, h1, -1.0, w);
-            multi_dotc(ctx, n, j + 1, V, w, h2);
-            multi_axpy(ctx, n, j + 1, V, h2, -1.0, w);
-            znrm2sq(ctx, n, w, nr);
-            lanczos_tridiag<<<1, 32, 0, ctx.stream>>>(j, alpha, beta, h1, h2, nr, which, tri, s);
-            NC_CHECK_LAUNCH();
-            ctx.launches++;
-            read_scalars(ctx, tri, sizeof(TriOut), &T);
-            jlast = j;
-            const double res = std::fabs(T.beta * T.s_last);
-            const double anorm = std::max(std::fabs(T.theta), eps23);
-            if (res <= tol_eff * anorm || j + 1 >= orth_dim) {
-                converged = true;
-                break;
-            }
-            if (j + 1 == m_max) break;
-            cplx* vn = V + (size_t)(j + 1) * n;
-            if (T.beta <= 1e3 * eps * std::max(T.tnorm, 1e-300)) {
-                // invariant subspace: continue with a fresh random direction
-                start_vector(vn, nullptr);
-                multi_dotc(ctx, n, j + 1, V, vn, h1);
-                multi_axpy(ctx, n, j + 1, V, h1, -1.0, vn);
-                multi_dotc(ctx, n, j + 1, V, vn, h1);
-                multi_axpy(ctx, n, j + 1, V, h1, -1.0, vn);
-                znrm2sq(ctx, n, vn, nr);
-                scale_by_inv_sqrt<<<g1(n), 256, 0, ctx.stream>>>(n, nr, vn, vn);
-                set_beta_zero<<<1, 1, 0, ctx.stream>>>(beta, j);
-                NC_CHECK_LAUNCH();
-                ctx.launches += 2;
-            } else {
-                scale_by_inv_sqrt<<<g1(n), 256, 0, ctx.stream>>>(n, nr, w, vn);
-                NC_CHECK_LAUNCH();
-                ctx.launches++;
-            }
-        }
-        // Ritz vector x = V s (normalised)
-        zfill(ctx, n, cmake(0, 0), result);
-        multi_axpy(ctx, n, jlast + 1, V, s, 1.0, result);
-        znrm2sq(ctx, n, result, nr);
-        if (converged) {
+        cplx* vj = V + (size_t)j * n;
+        heff_apply(ctx, bl, br, op, L, R, vj, w, ws);
+        filt.apply(ctx, n, w);
+        ++st.matvecs;
+        orthogonalise(w, j + 1);
+        fill_t_kernel<<<1, 32, 0, ctx.stream>>>(j, h1, h2, T);
+        NC_CHECK_LAUNCH();
+        ritz_kernel<<<1, 32, 0, ctx.stream>>>(j + 1, T, nr, which, ro, S, theta);
+        NC_CHECK_LAUNCH();
+        ctx.launches += 2;
+        RitzOut rr;
+        read_scalars(ctx, ro, sizeof(RitzOut), &rr);
+        const double anorm = std::max(std::fabs(rr.theta), eps23);
+        if (rr.res <= tol_eff * anorm || j + 1 >= orth_dim) {
+            // Ritz vector x = V s_0, cleaned of projector-space rounding and normalised
+            zfill(ctx, n, cmake(0, 0), result);
+            multi_axpy(ctx, n, j + 1, V, S, 1.0, result);
+            filt.apply(ctx, n, result);
+            znrm2sq(ctx, n, result, nr);
             scale_by_inv_sqrt<<<g1(n), 256, 0, ctx.stream>>>(n, nr, result, result);
             NC_CHECK_LAUNCH();
             ctx.launches++;
-            *eigenvalue = T.theta;
+            *eigenvalue = rr.theta;
             znrm2sq(ctx, n, result, nr);
             *normal = std::sqrt(read_scalar(ctx, nr).x);
             st.restarts = restarts;
             if (stats) *stats = st;
             return 0;
         }
-        ++restarts;
-        if (restarts >= maxit) {
-            st.restarts = restarts;
-            if (stats) *stats = st;
-            return -14;
+        if (j + 1 == m_max) {
+            // thick restart: keep the `keep` wanted Ritz vectors, continue from the residual
+            if (++restarts >= maxit) {
+                st.restarts = restarts;
+                if (stats) *stats = st;
+                return -14;
+            }
+            zgemm(zgemm_params(OP_N, OP_N, (int)std::min<long long>(n, 1LL << 30), keep, j + 1, V, n, S, j + 1, Y, n),
+                  ctx);
+            zcopy(ctx, (long long)keep * n, Y, V);
+            scale_by_inv_sqrt<<<g1(n), 256, 0, ctx.stream>>>(n, nr, w, V + (size_t)keep * n);
+            NC_CHECK_LAUNCH();
+            restart_t_kernel<<<1, 256, 0, ctx.stream>>>(keep, theta, T);
+            NC_CHECK_LAUNCH();
+            ctx.launches += 2;
+            j = keep;
+            continue;
         }
-        scale_by_inv_sqrt<<<g1(n), 256, 0, ctx.stream>>>(n, nr, result, V);
+        cplx* vn = V + (size_t)(j + 1) * n;
+        if (rr.beta <= 1e3 * eps * std::max(rr.tnorm, 1e-300)) {
+            // invariant subspace: continue with a fresh random direction
+            zrandom(ctx, n, seed++, vn);
+            filt.apply(ctx, n, vn);
+            orthogonalise(vn, j + 1);
+            scale_by_inv_sqrt<<<g1(n), 256, 0, ctx.stream>>>(n, nr, vn, vn);
+        } else {
+            scale_by_inv_sqrt<<<g1(n), 256, 0, ctx.stream>>>(n, nr, w, vn);
+        }
         NC_CHECK_LAUNCH();
         ctx.launches++;
+        ++j;
     }
 }
 

@@ -17,11 +17,16 @@ struct ZGemmParams {
     cplx* C; long long ldc, sC0, sC1;
     int nb0, batch;   // batch index b = b0 + nb0*b1; nb0 = 0: one level (b0 = b)
     cplx alpha, beta;
+    int kchunk, nsplit;  // split-K (set by zgemm(p, ctx); 0/1 = none)
+    cplx* ws;            // split-K partials
 };
 
 ZGemmParams zgemm_params(int opA, int opB, int M, int N, int K, const cplx* A, long long lda,
                          const cplx* B, long long ldb, cplx* C, long long ldc);
+// Plain launch on stream s (no split-K).
 void zgemm(const ZGemmParams& p, cudaStream_t s);
+// Launch with automatic split-K when the tile grid is small (workspace from ctx.arena).
+void zgemm(const ZGemmParams& p, Context& ctx);
 void scale_strided(const ZGemmParams& p, cudaStream_t s);
 
 // One MPO site on the device: W (d,d,nnz) column-major, idx (2,nnz) 1-based.
@@ -53,6 +58,10 @@ void overlap_site_from_state(Context& ctx, int br, int bl, int d, const cplx* S,
 // sum_{i,j,k} L(j,i,k) R(i,j,k) -> *result (device)
 void contract_exp_boundaries(Context& ctx, int b, int c, const cplx* L, const cplx* R,
                              cplx* result);
+
+// <psi|H|psi> at one site -> *result (device), via one H_eff product.
+void expectation_dev(Context& ctx, int bl, int br, const MpoSite& op, const cplx* L, const cplx* psi,
+                     const cplx* R, cplx* result);
 
 // ---- vector kernels (vector.cu) --------------------------------------------
 // out = permute(in) for 3-index column-major tensors: out axis k = in axis perm[k].
@@ -102,6 +111,22 @@ void unproject_unit(Context& ctx, const DevProjector& P, long long reduced_index
 // reflectors and R; returns the rank; swaps gets min(m,n) 1-based entries.
 int convert_vectors_to_reflectors_dev(Context& ctx, long long m, int n, cplx* A, cplx* tau_dev,
                                       std::vector<uint32_t>& swaps);
+
+// ---- QR and gauge moves (qr.cu) ----------------------------------------------
+// Householder QR of A (m x n, ld m, m >= n, m <= 2048): R left in the upper
+// triangle of A; optional explicit Q (m x n) and R (n x n, zeros below,
+// conjugated if conjR).
+void householder_qr(Context& ctx, int m, int n, cplx* A, cplx* Q, cplx* R, bool conjR);
+// A (bm,bl,dl) -> normA left-normalised; B (br,bm,dr) absorbs the factor.
+void gauge_right(Context& ctx, int bl, int bm, int br, int dl, int dr, const cplx* A, const cplx* B,
+                 cplx* normA, cplx* denormB);
+// B (br,bm,dr) -> normB right-normalised; A (bm,bl,dl) absorbs the factor.
+void gauge_left(Context& ctx, int bl, int bm, int br, int dl, int dr, const cplx* A, const cplx* B,
+                cplx* denormA, cplx* normB);
+void rand_norm_site(Context& ctx, int br, int bl, int d, uint64_t seed, cplx* out);
+void rand_unnorm_site(Context& ctx, int br, int bl, int d, uint64_t seed, cplx* out);
+void increase_bandwidth(Context& ctx, int bl, int bm, int br, int dl, int dr, int new_bm, uint64_t seed,
+                        const cplx* A, const cplx* B, cplx* outA, cplx* outB);
 
 // ---- Krylov eigensolver (lanczos.cu) -----------------------------------------
 // w -= sum_i h_i V_i and h = V^H w helpers (V: k columns of length n, ld n).

@@ -69,13 +69,25 @@ __global__ void __launch_bounds__(ZTile<BM, BN, BK, WM, WN, STAGES, OPA, OPB>::T
     const int bm0 = blockIdx.y * BM;
     const int bn0 = blockIdx.x * BN;
 
-    const long long b = blockIdx.z;
+    // blockIdx.z = b + batch * ks: batch entry b, K slice ks (split-K)
+    const long long b = blockIdx.z % p.batch;
+    const int ks = blockIdx.z / p.batch;
     const long long b0 = b % p.nb0, b1 = b / p.nb0;
     const cplx* __restrict__ A = p.A + b0 * p.sA0 + b1 * p.sA1;
     const cplx* __restrict__ B = p.B + b0 * p.sB0 + b1 * p.sB1;
     cplx* __restrict__ C = p.C + b0 * p.sC0 + b1 * p.sC1;
-    const int M = p.M, N = p.N, K = p.K;
-    const long long lda = p.lda, ldb = p.ldb, ldc = p.ldc;
+    const int M = p.M, N = p.N;
+    int K = p.K;
+    long long lda = p.lda, ldb = p.ldb, ldc = p.ldc;
+    if (p.kchunk > 0) {
+        const long long k0 = (long long)ks * p.kchunk;
+        K = (int)min((long long)p.kchunk, (long long)p.K - k0);
+        A += k0 * (T::A_KM ? lda : 1);
+        B += k0 * (T::B_NK ? 1 : ldb);
+        C = p.ws + ((long long)ks * p.batch + b) * (long long)M * N;  // raw partial, ld = M
+        ldc = M;
+    }
+    const bool raw = (p.kchunk > 0);
 
     auto load_tile = [&](int stage, int kt) {
         cplx* As = smem + stage * T::STAGE_ELEMS;
@@ -161,8 +173,8 @@ __global__ void __launch_bounds__(ZTile<BM, BN, BK, WM, WN, STAGES, OPA, OPB>::T
     }
     cp_async_wait<0>();
 
-    const cplx alpha = p.alpha, beta = p.beta;
-    const bool use_beta = (beta.x != 0.0 || beta.y != 0.0);
+    const cplx alpha = raw ? cmake(1, 0) : p.alpha, beta = p.beta;
+    const bool use_beta = !raw && (beta.x != 0.0 || beta.y != 0.0);
 #pragma unroll
     for (int i = 0; i < T::MT; ++i) {
         int m = bm0 + wm0 + 8 * i + g;
@@ -191,8 +203,8 @@ void launch_cfg(const ZGemmParams& p, cudaStream_t s) {
         NC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM));
         configured = true;
     }
-    dim3 grid(ceil_div(p.N, BN), ceil_div(p.M, BM), p.batch);
-    NC_ARG(p.batch <= 65535, "zgemm: batch too large");
+    dim3 grid(ceil_div(p.N, BN), ceil_div(p.M, BM), p.batch * p.nsplit);
+    NC_ARG((long long)p.batch * p.nsplit <= 65535, "zgemm: batch too large");
     kern<<<grid, T::THREADS, T::SMEM, s>>>(p);
     NC_CHECK_LAUNCH();
 }
@@ -200,19 +212,73 @@ void launch_cfg(const ZGemmParams& p, cudaStream_t s) {
 template <int OPA, int OPB>
 void launch_ops(const ZGemmParams& p, cudaStream_t s) {
     // Large problems: 128x64 tiles, 8 warps; small ones: 64x64, 4 warps.
-    long long tiles128 = (long long)ceil_div(p.M, 128) * ceil_div(p.N, 64) * p.batch;
+    long long tiles128 = (long long)ceil_div(p.M, 128) * ceil_div(p.N, 64) * p.batch * p.nsplit;
     if (p.M >= 128 && tiles128 >= 148)
         launch_cfg<128, 64, 16, 32, 32, 3, OPA, OPB>(p, s);
     else
         launch_cfg<64, 64, 16, 32, 32, 3, OPA, OPB>(p, s);
 }
 
+// C[b] = alpha * sum_ks ws[ks][b] + beta * C[b]
+__global__ void splitk_reduce_kernel(ZGemmParams p) {
+    const long long b = blockIdx.z;
+    cplx* C = p.C + (b % p.nb0) * p.sC0 + (b / p.nb0) * p.sC1;
+    const long long mn = (long long)p.M * p.N;
+    const bool use_beta = (p.beta.x != 0.0 || p.beta.y != 0.0);
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < mn;
+         e += (long long)gridDim.x * blockDim.x) {
+        cplx acc = cmake(0, 0);
+        for (int ks = 0; ks < p.nsplit; ++ks) acc = cadd(acc, p.ws[((long long)ks * p.batch + b) * mn + e]);
+        int m = (int)(e % p.M), n = (int)(e / p.M);
+        cplx* d = C + m + (long long)n * p.ldc;
+        cplx v = cmul(p.alpha, acc);
+        if (use_beta) v = cadd(v, cmul(p.beta, *d));
+        *d = v;
+    }
+}
+
 }  // namespace
+
+void zgemm(const ZGemmParams& p_in, Context& ctx) {
+    ZGemmParams p = p_in;
+    if (p.M <= 0 || p.N <= 0 || p.batch <= 0) return;
+    if (p.nb0 <= 0) p.nb0 = p.batch;
+    // Split K when the tile grid cannot fill the 148 SMs and K is long.
+    const long long tiles = (long long)ceil_div(p.M, 64) * ceil_div(p.N, 64) * p.batch;
+    int nsplit = 1;
+    if (p.K >= 256 && tiles < 2 * 148) {
+        nsplit = (int)std::min<long long>((2 * 148 + tiles - 1) / tiles, p.K / 128);
+        nsplit = std::max(1, std::min(nsplit, 32));
+    }
+    if (nsplit <= 1) {
+        zgemm(p, ctx.stream);
+        ctx.launches++;
+        return;
+    }
+    int kchunk = (int)(((p.K + nsplit - 1) / nsplit + 15) / 16 * 16);
+    nsplit = (p.K + kchunk - 1) / kchunk;
+    ArenaFrame f(ctx.arena);
+    const long long mn = (long long)p.M * p.N;
+    cplx* ws = ctx.arena.alloc_n<cplx>((size_t)mn * p.batch * nsplit);
+    ZGemmParams q = p;
+    q.kchunk = kchunk;
+    q.nsplit = nsplit;
+    q.ws = ws;
+    zgemm(q, ctx.stream);
+    ZGemmParams r = p;
+    r.nsplit = nsplit;
+    r.ws = ws;
+    dim3 grid(std::min<unsigned>(ceil_div((size_t)mn, 256), 1024), 1, p.batch);
+    splitk_reduce_kernel<<<grid, 256, 0, ctx.stream>>>(r);
+    NC_CHECK_LAUNCH();
+    ctx.launches += 2;
+}
 
 void zgemm(const ZGemmParams& p_in, cudaStream_t s) {
     ZGemmParams p = p_in;
     if (p.M <= 0 || p.N <= 0 || p.batch <= 0) return;
     if (p.nb0 <= 0) p.nb0 = p.batch;  // single-level batch: every index on level 0
+    if (p.nsplit <= 0 || p.kchunk <= 0) { p.nsplit = 1; p.kchunk = 0; }
     if (p.K <= 0) {
         // C = beta * C
         scale_strided(p, s);
@@ -259,6 +325,7 @@ ZGemmParams zgemm_params(int opA, int opB, int M, int N, int K, const cplx* A, l
     p.C = C; p.ldc = ldc; p.sC0 = 0; p.sC1 = 0;
     p.nb0 = 0; p.batch = 1;  // nb0 = 0: single-level batch over the *0 strides
     p.alpha = cmake(1, 0); p.beta = cmake(0, 0);
+    p.kchunk = 0; p.nsplit = 1; p.ws = nullptr;
     return p;
 }
 

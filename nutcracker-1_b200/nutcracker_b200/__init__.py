@@ -246,9 +246,91 @@ class _CoreSolver:
         return int(rank.value), refl, coeff[:k], swaps[:k]
 
 
+    # -- gauge moves (core.cpp:570-765) -----------------------------------
+    @staticmethod
+    def norm_denorm_going_left(bl, bm, br, dl, dr, A, B):
+        """Returns (info, denormalized A (bm,bl,dl), normalized B (br,bm,dr))."""
+        A, B = _F(A), _F(B)
+        oA = np.zeros((bm, bl, dl), C128, order="F")
+        oB = np.zeros((br, bm, dr), C128, order="F")
+        info = lib.norm_denorm_going_left_(_u(bl), _u(bm), _u(br), _u(dl), _u(dr), _c(A), _c(B), _c(oA), _c(oB))
+        _check()
+        return info, oA, oB
+
+    @staticmethod
+    def norm_denorm_going_right(bl, bm, br, dl, dr, A, B):
+        """Returns (info, normalized A (bm,bl,dl), denormalized B (br,bm,dr))."""
+        A, B = _F(A), _F(B)
+        oA = np.zeros((bm, bl, dl), C128, order="F")
+        oB = np.zeros((br, bm, dr), C128, order="F")
+        info = lib.norm_denorm_going_right_(_u(bl), _u(bm), _u(br), _u(dl), _u(dr), _c(A), _c(B), _c(oA), _c(oB))
+        _check()
+        return info, oA, oB
+
+    @staticmethod
+    def norm_for_left(br, bl, d, S):
+        S = _F(S)
+        out = np.zeros((br, bl, d), C128, order="F")
+        info = lib.norm_for_left_(_u(br), _u(bl), _u(d), _c(S), _c(out))
+        _check()
+        return info, out
+
+    @staticmethod
+    def norm_for_right(br, bl, d, S):
+        S = _F(S)
+        out = np.zeros((br, bl, d), C128, order="F")
+        info = lib.norm_for_right_(_u(br), _u(bl), _u(d), _c(S), _c(out))
+        _check()
+        return info, out
+
+    @staticmethod
+    def increase_bandwidth_between(bl, bm, br, dl, dr, new_bm, A, B):
+        A, B = _F(A), _F(B)
+        oA = np.zeros((new_bm, bl, dl), C128, order="F")
+        oB = np.zeros((br, new_bm, dr), C128, order="F")
+        info = lib.increase_bandwidth_between_(_u(bl), _u(bm), _u(br), _u(dl), _u(dr), _u(new_bm), _c(A), _c(B),
+                                               _c(oA), _c(oB))
+        _check()
+        return info, oA, oB
+
+    @staticmethod
+    def rand_norm_state_site_tensor(br, bl, d):
+        out = np.zeros((br, bl, d), C128, order="F")
+        lib.rand_norm_state_site_tensor_(_u(br), _u(bl), _u(d), _c(out))
+        _check()
+        return out
+
+    @staticmethod
+    def rand_unnorm_state_site_tensor(br, bl, d):
+        out = np.zeros((br, bl, d), C128, order="F")
+        lib.rand_unnorm_state_site_tensor_(_u(br), _u(bl), _u(d), _c(out))
+        _check()
+        return out
+
+    @staticmethod
+    def form_norm_overlap_tensors(bl, bm, br, dl, dr, S1, S2):
+        S1, S2 = _F(S1), _F(S2)
+        lno = np.zeros((bl, dl, bm), C128, order="F")
+        uno = np.zeros((bl, dl, bm), C128, order="F")
+        dS2 = np.zeros((br, bm, dr), C128, order="F")
+        rno = np.zeros((bm, dr, br), C128, order="F")
+        lib.form_norm_overlap_tensors_(_u(bl), _u(bm), _u(br), _u(dl), _u(dr), _c(S1), _c(S2), _c(lno), _c(uno),
+                                       _c(dS2), _c(rno))
+        _check()
+        return lno, uno, dS2, rno
+
+
 for _name in ("optimize", "convert_vectors_to_reflectors", "filter_components_outside_orthog",
-              "compute_overlap_with_projectors", "random_projector_matrix"):
+              "compute_overlap_with_projectors", "random_projector_matrix", "norm_denorm_going_left",
+              "norm_denorm_going_right", "norm_for_left", "norm_for_right", "increase_bandwidth_between",
+              "rand_norm_state_site_tensor", "rand_unnorm_state_site_tensor", "form_norm_overlap_tensors"):
     setattr(Core, _name, getattr(_CoreSolver, _name))
+
+lib.norm_denorm_going_left_.restype = ct.c_int32
+lib.norm_denorm_going_right_.restype = ct.c_int32
+lib.norm_for_left_.restype = ct.c_int32
+lib.norm_for_right_.restype = ct.c_int32
+lib.increase_bandwidth_between_.restype = ct.c_int32
 
 
 def set_krylov_dimension(m):

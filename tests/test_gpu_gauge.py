@@ -1,0 +1,130 @@
+"""GPU parity: gauge moves, bandwidth growth, random sites, projector sites.
+
+The device gauge is a Householder-QR factor instead of the reference's SVD
+polar factor (core.f95:2708-2960), so outputs are compared through the
+gauge-invariant quantities the reference's own tests use (tests/states.cpp,
+tests/chain.cpp:143-169): the contracted two-site tensor, orthonormality of
+the normalised site, and the state itself.  Tolerance 1e-12 relative.
+"""
+import numpy as np
+import pytest
+
+from gpu_util import rand_c, rel_err
+from oracle import core
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def nb():
+    import nutcracker_b200
+    return nutcracker_b200
+
+
+def pair(A, B):
+    """Two-site tensor sum_m A(m,l,s) B(r,m,t) -> (l,s,r,t)."""
+    return np.einsum("mls,rmt->lsrt", A, B)
+
+
+def left_normal_err(S):
+    br, bl, d = S.shape
+    M = np.reshape(S, (br, bl * d), order="F")
+    return np.abs(M @ M.conj().T - np.eye(br)).max()
+
+
+def right_normal_err(S):
+    br, bl, d = S.shape
+    M = np.reshape(np.transpose(S, (1, 0, 2)), (bl, br * d), order="F")
+    return np.abs(M @ M.conj().T - np.eye(bl)).max()
+
+
+DIMS = [(1, 2, 2, 2, 2), (2, 4, 8, 2, 2), (3, 5, 4, 2, 3), (16, 32, 16, 2, 2), (40, 60, 33, 2, 2),
+        (100, 200, 100, 2, 2), (256, 300, 256, 2, 2), (120, 250, 250, 3, 3)]
+
+
+@pytest.mark.parametrize("dims", DIMS, ids=lambda d: "x".join(map(str, d)))
+def test_norm_denorm_going_right(nb, dims):
+    bl, bm, br, dl, dr = dims
+    if bl * dl < bm:
+        pytest.skip("not normalisable")
+    rng = np.random.default_rng(sum(dims))
+    A = rand_c(rng, (bm, bl, dl)); B = rand_c(rng, (br, bm, dr))
+    info, nA, dB = nb.Core.norm_denorm_going_right(bl, bm, br, dl, dr, A, B)
+    assert info == 0
+    assert left_normal_err(nA) < 1e-12
+    assert rel_err(pair(nA, dB), pair(A, B)) < 1e-12
+    # same state as the reference's polar move
+    _, rA, rB = core.norm_denorm_going_right(bl, bm, br, dl, dr, A, B)
+    assert rel_err(pair(nA, dB), pair(rA, rB)) < 1e-12
+
+
+@pytest.mark.parametrize("dims", DIMS, ids=lambda d: "x".join(map(str, d)))
+def test_norm_denorm_going_left(nb, dims):
+    bl, bm, br, dl, dr = dims
+    if br * dr < bm:
+        pytest.skip("not normalisable")
+    rng = np.random.default_rng(7 + sum(dims))
+    A = rand_c(rng, (bm, bl, dl)); B = rand_c(rng, (br, bm, dr))
+    info, dA, nB = nb.Core.norm_denorm_going_left(bl, bm, br, dl, dr, A, B)
+    assert info == 0
+    assert right_normal_err(nB) < 1e-12
+    assert rel_err(pair(dA, nB), pair(A, B)) < 1e-12
+
+
+def test_rank_deficient_gauge(nb):
+    """A site of rank 3 < bm still yields an exactly left-normalised factor."""
+    rng = np.random.default_rng(5)
+    bl, bm, br, d = 20, 16, 16, 2
+    U = rand_c(rng, (bm, 3)); V = rand_c(rng, (3, bl * d))
+    A = np.asfortranarray(np.reshape(U @ V, (bm, bl, d), order="F"))
+    B = rand_c(rng, (br, bm, d))
+    info, nA, dB = nb.Core.norm_denorm_going_right(bl, bm, br, d, d, A, B)
+    assert info == 0 and left_normal_err(nA) < 1e-12
+    assert rel_err(pair(nA, dB), pair(A, B)) < 1e-12
+
+
+def test_norm_for_left_right(nb):
+    rng = np.random.default_rng(9)
+    S = rand_c(rng, (12, 10, 2))
+    info, L = nb.Core.norm_for_left(12, 10, 2, S)
+    assert info == 0 and left_normal_err(L) < 1e-12
+    # same row space as the reference's polar factor
+    _, Lr = core.norm_for_left(12, 10, 2, S)
+    P = lambda X: np.reshape(X, (12, 20), order="F").conj().T @ np.reshape(X, (12, 20), order="F")
+    assert rel_err(P(L), P(Lr)) < 1e-12
+    S = rand_c(rng, (10, 12, 2))
+    info, R = nb.Core.norm_for_right(10, 12, 2, S)
+    assert info == 0 and right_normal_err(R) < 1e-12
+
+
+@pytest.mark.parametrize("dims", [(2, 2, 4, 2, 2, 4), (4, 6, 8, 2, 2, 8), (16, 20, 32, 2, 2, 32), (9, 9, 9, 3, 3, 20)])
+def test_increase_bandwidth_between(nb, dims):
+    bl, bm, br, dl, dr, nbm = dims
+    rng = np.random.default_rng(sum(dims))
+    A = rand_c(rng, (bm, bl, dl)); B = rand_c(rng, (br, bm, dr))
+    info, oA, oB = nb.Core.increase_bandwidth_between(bl, bm, br, dl, dr, nbm, A, B)
+    assert info == 0 and oA.shape == (nbm, bl, dl) and oB.shape == (br, nbm, dr)
+    assert right_normal_err(oB) < 1e-12
+    assert rel_err(pair(oA, oB), pair(A, B)) < 1e-12
+
+
+def test_random_sites(nb):
+    S = nb.Core.rand_norm_state_site_tensor(8, 16, 2)
+    assert right_normal_err(S) < 1e-12
+    T = nb.Core.rand_unnorm_state_site_tensor(8, 16, 2)
+    assert abs(np.linalg.norm(T) - 1) < 1e-14
+    U = nb.Core.rand_unnorm_state_site_tensor(8, 16, 2)
+    assert rel_err(T, U) > 0.1  # fresh draws
+
+
+def test_form_norm_overlap_tensors(nb):
+    rng = np.random.default_rng(12)
+    bl, bm, br, dl, dr = 4, 8, 6, 2, 2
+    S1 = rand_c(rng, (bm, bl, dl))
+    _, S2 = core.norm_for_right(br, bm, dr, rand_c(rng, (br, bm, dr)))
+    lno, uno, dS2, rno = nb.Core.form_norm_overlap_tensors(bl, bm, br, dl, dr, S1, S2)
+    rl, ru, rd, rr = core.form_norm_overlap_tensors(bl, bm, br, dl, dr, S1, S2)
+    assert rel_err(uno, ru) == 0 and rel_err(rno, rr) == 0
+    # the left-normalised overlap site and the denormalised site 2 carry the same pair
+    back = lambda O: np.conj(np.transpose(O, (2, 0, 1)))  # overlap (bl,d,br) -> state (br,bl,d)
+    assert rel_err(pair(back(lno), dS2), pair(back(rl), rd)) < 1e-12
