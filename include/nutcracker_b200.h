@@ -44,6 +44,12 @@ int nc_set_stream(void* stream);
 int nc_use_own_stream(void);
 /* Wait for this thread's stream.  Returns a status code. */
 int nc_synchronize(void);
+/* Start timing every complex GEMM of at least `min_flops` algorithmic flops
+   with CUDA events on this thread's stream. */
+int nc_profile_begin(double min_flops);
+/* Stop timing; report the number of timed GEMMs, their summed device time
+   (ms) and summed algorithmic flops (8*M*N*K per complex product). */
+int nc_profile_end(uint64_t* launches, double* total_ms, double* total_flops);
 
 /* Device-pointer effective-Hamiltonian product y = H_eff x for one site
    (the strategy-3 `operate_on` of core.f95:2529-2556 without projectors):
@@ -54,7 +60,7 @@ int nc_heff_apply_dev(uint32_t bl, uint32_t br, uint32_t cl, uint32_t cr, uint32
                       const uint32_t* idx_dev, const void* W_dev, const void* L_dev,
                       const void* R_dev, const void* x_dev, void* y_dev);
 
-/* ---- Level 0: contractions (sources/common/core.cpp:33-420) ------------- */
+/* ---- Level 0: contractions (sources/common/core.cpp:33-526) ------------- */
 
 /* core.cpp:33-45 (compute_expectation_): <psi|H|psi> at one site. */
 void compute_expectation_(const uint32_t* bl, const uint32_t* br, const uint32_t* cl,
@@ -74,17 +80,17 @@ void compute_optimization_matrix_(const uint32_t* bl, const uint32_t* br, const 
                                   const nc_complex* right_environment,
                                   nc_complex* optimization_matrix);
 
-/* core.cpp:145-150 (construct_left_exp_boundary_). */
+/* core.cpp:139-144 (construct_left_exp_boundary_). */
 void construct_left_exp_boundary_(const uint32_t* b, const uint32_t* c,
                                   const nc_complex* state_boundary,
                                   const nc_complex* operator_boundary,
                                   nc_complex* left_expectation_boundary);
-/* core.cpp:165-170 (construct_right_exp_boundary_). */
+/* core.cpp:161-166 (construct_right_exp_boundary_). */
 void construct_right_exp_boundary_(const uint32_t* b, const uint32_t* c,
                                    const nc_complex* state_boundary,
                                    const nc_complex* operator_boundary,
                                    nc_complex* right_expectation_boundary);
-/* core.cpp:185-191 (contract_expectation_boundaries_). */
+/* core.cpp:183-189 (contract_expectation_boundaries_). */
 void contract_expectation_boundaries_(const uint32_t* b, const uint32_t* c,
                                       const nc_complex* left_boundary,
                                       const nc_complex* right_boundary, nc_complex* expectation);
@@ -95,39 +101,39 @@ void contract_sos_left_(const uint32_t* bl, const uint32_t* br, const uint32_t* 
                         const uint32_t* number_of_matrices, const uint32_t* sparse_operator_indices,
                         const nc_complex* sparse_operator_matrices,
                         const nc_complex* state_site_tensor, nc_complex* new_left_environment);
-/* core.cpp:274-286 (contract_sos_right_): new right environment (bl,bl,cl). */
+/* core.cpp:272-284 (contract_sos_right_): new right environment (bl,bl,cl). */
 void contract_sos_right_(const uint32_t* bl, const uint32_t* br, const uint32_t* cl,
                          const uint32_t* cr, const uint32_t* d, const nc_complex* right_environment,
                          const uint32_t* number_of_matrices, const uint32_t* sparse_operator_indices,
                          const nc_complex* sparse_operator_matrices,
                          const nc_complex* state_site_tensor, nc_complex* new_right_environment);
-/* core.cpp:313-322 (contract_vs_left_). */
+/* core.cpp:309-318 (contract_vs_left_). */
 void contract_vs_left_(const uint32_t* b_left_old, const uint32_t* b_right_old,
                        const uint32_t* b_left_new, const uint32_t* b_right_new, const uint32_t* d,
                        const nc_complex* left_environment,
                        const nc_complex* normalized_projector_site_tensor,
                        const nc_complex* normalized_state_site_tensor,
                        nc_complex* new_left_environment);
-/* core.cpp:347-356 (contract_vs_right_). */
+/* core.cpp:340-349 (contract_vs_right_). */
 void contract_vs_right_(const uint32_t* b_left_old, const uint32_t* b_right_old,
                         const uint32_t* b_left_new, const uint32_t* b_right_new, const uint32_t* d,
                         const nc_complex* right_environment,
                         const nc_complex* normalized_projector_site_tensor,
                         const nc_complex* normalized_state_site_tensor,
                         nc_complex* new_right_environment);
-/* core.cpp:529-538 (form_overlap_vector_). */
+/* core.cpp:517-526 (form_overlap_vector_). */
 void form_overlap_vector_(const uint32_t* b_left_old, const uint32_t* b_right_old,
                           const uint32_t* b_left_new, const uint32_t* b_right_new,
                           const uint32_t* d, const nc_complex* left_environment,
                           const nc_complex* right_environment,
                           const nc_complex* unnormalized_projector_site_tensor,
                           nc_complex* overlap_vector);
-/* core.cpp:510-515 (form_overlap_site_tensor_). */
+/* core.cpp:498-504 (form_overlap_site_tensor_). */
 void form_overlap_site_tensor_(const uint32_t* br, const uint32_t* bl, const uint32_t* d,
                                const nc_complex* state_site_tensor,
                                nc_complex* overlap_site_tensor);
 
-/* ---- Level 0: site eigen-solve and projectors (core.cpp:420-760) -------- */
+/* ---- Level 0: site eigen-solve and projectors (core.cpp:109-441, 676-774) -------- */
 
 /* core.cpp:676-693 (optimize_): the site eigen-solve.  Returns the
    reference's info code: 0 success, 5 orthogonal dimension too large,
@@ -148,12 +154,12 @@ uint32_t optimize_(const uint32_t* bl, const uint32_t* br, const uint32_t* cl, c
                    const double* tol, uint32_t* number_of_iterations, const nc_complex* guess,
                    nc_complex* result, nc_complex* eigenvalue, double* normal);
 
-/* core.cpp:370-391 (convert_vectors_to_reflectors_): pivoted Householder QR
+/* core.cpp:371-378 (convert_vectors_to_reflectors_): pivoted Householder QR
    of `m` overlap vectors of length `n`, in place; rank and swaps out. */
 void convert_vectors_to_reflectors_(const uint32_t* n, const uint32_t* m, nc_complex* vectors,
                                     uint32_t* rank, nc_complex* coefficients, uint32_t* swaps);
 
-/* core.cpp:425-449 (filter_components_outside_orthog_): output = the input
+/* core.cpp:431-441 (filter_components_outside_orthog_): output = the input
    with its components in the projector space removed. */
 void filter_components_outside_orthog_(const uint32_t* full_space_dimension,
                                        const uint32_t* number_of_projectors,
@@ -163,7 +169,7 @@ void filter_components_outside_orthog_(const uint32_t* full_space_dimension,
                                        const uint32_t* swaps, const nc_complex* input,
                                        nc_complex* output);
 
-/* core.cpp:107-134 (compute_overlap_with_projectors_): the Fortran routine
+/* core.cpp:109-118 (compute_overlap_with_projectors_): the Fortran routine
    writes a real overlap; it is returned in overlap->re with overlap->im = 0. */
 void compute_overlap_with_projectors_(const uint32_t* number_of_projectors,
                                       const uint32_t* number_of_reflectors,
@@ -171,7 +177,7 @@ void compute_overlap_with_projectors_(const uint32_t* number_of_projectors,
                                       const uint32_t* swaps, const uint32_t* vector_size,
                                       const nc_complex* vector, nc_complex* overlap);
 
-/* core.cpp:766-781 (random_projector_matrix_): reflectors of random
+/* core.cpp:769-774 (random_projector_matrix_): reflectors of random
    projector vectors (seeded device generator instead of gfortran rand()). */
 void random_projector_matrix_(const uint32_t* projector_length, const uint32_t* number_of_projectors,
                               uint32_t* rank, nc_complex* reflectors, nc_complex* coefficients,
@@ -180,7 +186,7 @@ void random_projector_matrix_(const uint32_t* projector_length, const uint32_t* 
 /* Lanczos basis size used by optimize_ on this thread (default 24). */
 int nc_set_krylov_dimension(int m);
 
-/* ---- Level 0: gauge moves and random sites (core.cpp:580-680, 736-765) --
+/* ---- Level 0: gauge moves and random sites (core.cpp:463-662, 735-757) --
    The device path uses a Householder-QR gauge (A = P Q with Q row-
    orthonormal) instead of the reference's SVD polar factor; the normalised
    and denormalised outputs differ from the reference element-wise by a
@@ -188,7 +194,7 @@ int nc_set_krylov_dimension(int m);
    energies, environments, overlaps) is identical.  Return 0 on success,
    a nonzero status otherwise. */
 
-/* core.cpp:601-628 (norm_denorm_going_left_): site_tensor_to_normalize
+/* core.cpp:580-589 (norm_denorm_going_left_): site_tensor_to_normalize
    (br,bm,dr) becomes right-normalised, site_tensor_to_denormalize (bm,bl,dl)
    absorbs the factor. */
 int32_t norm_denorm_going_left_(const uint32_t* bl, const uint32_t* bm, const uint32_t* br,
@@ -197,7 +203,7 @@ int32_t norm_denorm_going_left_(const uint32_t* bl, const uint32_t* bm, const ui
                                 const nc_complex* site_tensor_to_normalize,
                                 nc_complex* denormalized_site_tensor,
                                 nc_complex* normalized_site_tensor);
-/* core.cpp:632-659 (norm_denorm_going_right_): site_tensor_to_normalize
+/* core.cpp:609-618 (norm_denorm_going_right_): site_tensor_to_normalize
    (bm,bl,dl) becomes left-normalised, site_tensor_to_denormalize (br,bm,dr)
    absorbs the factor. */
 int32_t norm_denorm_going_right_(const uint32_t* bl, const uint32_t* bm, const uint32_t* br,
@@ -206,13 +212,13 @@ int32_t norm_denorm_going_right_(const uint32_t* bl, const uint32_t* bm, const u
                                  const nc_complex* site_tensor_to_denormalize,
                                  nc_complex* normalized_site_tensor,
                                  nc_complex* denormalized_site_tensor);
-/* core.cpp:663-677 (norm_for_left_): left-normalised factor of a site. */
+/* core.cpp:638-643 (norm_for_left_): left-normalised factor of a site. */
 int32_t norm_for_left_(const uint32_t* br, const uint32_t* bl, const uint32_t* d,
                        const nc_complex* site_tensor, nc_complex* normalized_site_tensor);
-/* core.cpp:681-695 (norm_for_right_): right-normalised factor of a site. */
+/* core.cpp:657-662 (norm_for_right_): right-normalised factor of a site. */
 int32_t norm_for_right_(const uint32_t* br, const uint32_t* bl, const uint32_t* d,
                         const nc_complex* site_tensor, nc_complex* normalized_site_tensor);
-/* core.cpp:570-599 (increase_bandwidth_between_): grow the bond between a
+/* core.cpp:548-559 (increase_bandwidth_between_): grow the bond between a
    normalised site (bm,bl,dl) and its right neighbour (br,bm,dr) to new_bm;
    outputs (new_bm,bl,dl) carrying the weight and (br,new_bm,dr) right-
    normalised. */
@@ -222,14 +228,14 @@ int32_t increase_bandwidth_between_(const uint32_t* bl, const uint32_t* bm, cons
                                     const nc_complex* site_tensor_to_denormalize,
                                     nc_complex* normalized_site_tensor,
                                     nc_complex* denormalized_site_tensor);
-/* core.cpp:736-747 (rand_norm_state_site_tensor_): right-normalised random
+/* core.cpp:735-740 (rand_norm_state_site_tensor_): right-normalised random
    site (seeded device generator). */
 void rand_norm_state_site_tensor_(const uint32_t* br, const uint32_t* bl, const uint32_t* d,
                                   nc_complex* state_site_tensor);
-/* core.cpp:751-762 (rand_unnorm_state_site_tensor_): random site of unit norm. */
+/* core.cpp:752-757 (rand_unnorm_state_site_tensor_): random site of unit norm. */
 void rand_unnorm_state_site_tensor_(const uint32_t* br, const uint32_t* bl, const uint32_t* d,
                                     nc_complex* state_site_tensor);
-/* core.cpp:463-489 (form_norm_overlap_tensors_): the projector sites of one
+/* core.cpp:463-475 (form_norm_overlap_tensors_): the projector sites of one
    bond (left-normalised and centre overlap sites of site 1, site 2 with the
    factor absorbed, right-normalised overlap site of site 2). */
 void form_norm_overlap_tensors_(const uint32_t* bl, const uint32_t* bm, const uint32_t* br,

@@ -122,6 +122,36 @@ int nc_use_own_stream(void) {
     return g_status;
 }
 
+int nc_profile_begin(double min_flops) {
+    NC_ABI_BEGIN
+    Context& ctx = Context::get();
+    ctx.profile = true;
+    ctx.profile_min_flops = min_flops;
+    ctx.prof_used = 0;
+    NC_ABI_END
+    return g_status;
+}
+
+int nc_profile_end(uint64_t* launches, double* total_ms, double* total_flops) {
+    NC_ABI_BEGIN
+    Context& ctx = Context::get();
+    NC_CUDA(cudaStreamSynchronize(ctx.stream));
+    double ms = 0, fl = 0;
+    for (size_t i = 0; i < ctx.prof_used; ++i) {
+        float t = 0;
+        NC_CUDA(cudaEventElapsedTime(&t, ctx.prof_start[i], ctx.prof_stop[i]));
+        ms += t;
+        fl += ctx.prof_flops[i];
+    }
+    *launches = ctx.prof_used;
+    *total_ms = ms;
+    *total_flops = fl;
+    ctx.profile = false;
+    ctx.prof_used = 0;
+    NC_ABI_END
+    return g_status;
+}
+
 int nc_synchronize(void) {
     NC_ABI_BEGIN
     NC_CUDA(cudaStreamSynchronize(Context::get().stream));

@@ -97,6 +97,13 @@ struct Context {
     size_t pinned_bytes = 0;
     uint64_t launches = 0;   // kernels launched by this library on this context
     int krylov_dim = 24;     // Lanczos basis size before a restart
+    // Kernel timing (nc_profile_begin/end): CUDA events around every complex
+    // GEMM of at least profile_min_flops, on the launching stream.
+    bool profile = false;
+    double profile_min_flops = 1e9;
+    std::vector<cudaEvent_t> prof_start, prof_stop;
+    std::vector<double> prof_flops;
+    size_t prof_used = 0;
     Context();
     ~Context();
     static Context& get();   // thread-local default context

@@ -239,7 +239,33 @@ __global__ void splitk_reduce_kernel(ZGemmParams p) {
 
 }  // namespace
 
-void zgemm(const ZGemmParams& p_in, Context& ctx) {
+namespace {
+void zgemm_ctx(const ZGemmParams& p_in, Context& ctx);
+}
+
+void zgemm(const ZGemmParams& p, Context& ctx) {
+    const double flops = 8.0 * p.M * (double)p.N * p.K * p.batch;
+    if (!ctx.profile || flops < ctx.profile_min_flops) {
+        zgemm_ctx(p, ctx);
+        return;
+    }
+    if (ctx.prof_used == ctx.prof_start.size()) {
+        cudaEvent_t a, b;
+        NC_CUDA(cudaEventCreate(&a));
+        NC_CUDA(cudaEventCreate(&b));
+        ctx.prof_start.push_back(a);
+        ctx.prof_stop.push_back(b);
+        ctx.prof_flops.push_back(0);
+    }
+    const size_t i = ctx.prof_used++;
+    ctx.prof_flops[i] = flops;
+    NC_CUDA(cudaEventRecord(ctx.prof_start[i], ctx.stream));
+    zgemm_ctx(p, ctx);
+    NC_CUDA(cudaEventRecord(ctx.prof_stop[i], ctx.stream));
+}
+
+namespace {
+void zgemm_ctx(const ZGemmParams& p_in, Context& ctx) {
     ZGemmParams p = p_in;
     if (p.M <= 0 || p.N <= 0 || p.batch <= 0) return;
     if (p.nb0 <= 0) p.nb0 = p.batch;
@@ -273,6 +299,7 @@ void zgemm(const ZGemmParams& p_in, Context& ctx) {
     NC_CHECK_LAUNCH();
     ctx.launches += 2;
 }
+}  // namespace
 
 void zgemm(const ZGemmParams& p_in, cudaStream_t s) {
     ZGemmParams p = p_in;
