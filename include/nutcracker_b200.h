@@ -60,6 +60,24 @@ int nc_heff_apply_dev(uint32_t bl, uint32_t br, uint32_t cl, uint32_t cr, uint32
                       const uint32_t* idx_dev, const void* W_dev, const void* L_dev,
                       const void* R_dev, const void* x_dev, void* y_dev);
 
+/* No counterpart in the reference.  The same H_eff product as
+   nc_heff_apply_dev for callers that cannot let the library allocate
+   device memory (a fixed memory budget, or code where a cudaMalloc/cudaFree
+   would stall the device): it allocates nothing and takes its scratch from
+   one fixed 64 MiB device array compiled into the library, which every GPU
+   that loads the library holds until exit.  A call needs
+   16*(br*bl*cl*d + br*cr*bl*d) bytes of it; larger calls return an error
+   and launch nothing.  Work is enqueued on `stream` (a cudaStream_t, NULL =
+   legacy default stream).  The first call on each device looks the array's
+   device address up (cudaGetSymbolAddress); make it before any stream
+   capture.  All calls share the array and each rewrites it completely, so
+   nothing needs clearing, but calls that overlap on the GPU race: order them
+   on one stream.  Returns a status code. */
+int nc_heff_apply_dev_noalloc(uint32_t bl, uint32_t br, uint32_t cl, uint32_t cr, uint32_t d,
+                              uint32_t nnz, const uint32_t* idx_dev, const void* W_dev,
+                              const void* L_dev, const void* R_dev, const void* x_dev,
+                              void* y_dev, void* stream);
+
 /* ---- Level 0: contractions (sources/common/core.cpp:33-526) ------------- */
 
 /* core.cpp:33-45 (compute_expectation_): <psi|H|psi> at one site. */

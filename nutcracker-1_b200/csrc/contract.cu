@@ -149,6 +149,26 @@ void heff_apply(Context& ctx, int bl, int br, const MpoSite& op, const cplx* L, 
     zgemm(p, ctx);
 }
 
+void heff_apply_stream(cudaStream_t s, int bl, int br, const MpoSite& op, const cplx* L, const cplx* R,
+                       const cplx* x, cplx* y, cplx* ws) {
+    // Same three steps as heff_apply, launched directly on `s` with the
+    // caller's scratch `ws` and no split-K (nothing is allocated).
+    check_op(op);
+    cplx* T = ws;
+    cplx* U = ws + (size_t)br * bl * op.cl * op.d;
+    ZGemmParams a = zgemm_params(OP_N, OP_N, br, bl * op.cl, bl, x, br, L, bl, T, br);
+    a.batch = op.d;
+    a.sA0 = (long long)br * bl; a.sB0 = 0; a.sC0 = (long long)br * bl * op.cl;
+    zgemm(a, s);
+    long long total = (long long)br * op.cr * bl * op.d;
+    mix_left_kernel<<<grid_for(total, 256), 256, 0, s>>>(br, bl, op.cl, op.cr, op.d, op.nnz, op.idx, op.W, T, U);
+    NC_CHECK_LAUNCH();
+    ZGemmParams c = zgemm_params(OP_N, OP_N, br, bl, br * op.cr, R, br, U, (long long)br * op.cr, y, br);
+    c.batch = op.d;
+    c.sA0 = 0; c.sB0 = (long long)br * op.cr * bl; c.sC0 = (long long)br * bl;
+    zgemm(c, s);
+}
+
 void sos_left(Context& ctx, int bl, int br, const MpoSite& op, const cplx* L, const cplx* psi,
               cplx* Lnew) {
     check_op(op);

@@ -41,6 +41,9 @@ size_t heff_workspace_elems(int bl, int br, const MpoSite& op);
 // y = H_eff x for x, y of shape (br,bl,d).  ws: heff_workspace_elems complex.
 void heff_apply(Context& ctx, int bl, int br, const MpoSite& op, const cplx* L, const cplx* R,
                 const cplx* x, cplx* y, cplx* ws);
+// The same product launched on stream s with caller-provided scratch only.
+void heff_apply_stream(cudaStream_t s, int bl, int br, const MpoSite& op, const cplx* L, const cplx* R,
+                       const cplx* x, cplx* y, cplx* ws);
 // New left environment (br,br,cr) from L (bl,bl,cl) and psi (br,bl,d).
 void sos_left(Context& ctx, int bl, int br, const MpoSite& op, const cplx* L, const cplx* psi,
               cplx* Lnew);
