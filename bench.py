@@ -61,6 +61,10 @@ def parse():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--phases", action="store_true",
+                    help="synchronise and time each sweep phase (diagnostics; slows the sweep slightly)")
+    ap.add_argument("--gauge-only", action="store_true",
+                    help="time only the Householder-QR gauge move of a chi x chi site (kernel profiling)")
     ap.add_argument("--heff-only", action="store_true",
                     help="time only the effective-Hamiltonian product at --chi (kernel profiling)")
     return ap.parse_args()
@@ -110,6 +114,26 @@ def run_heff_only(args):
     t = e0.elapsed_time(e1) / 1e3 / args.steps
     flops = 8 * d * chi * chi * (cl * chi + cr * chi) + 8 * op.nnz * d * d * chi * chi
     print(json.dumps({"heff_chi": chi, "ms": t * 1e3, "tflops": flops / t / 1e12}), flush=True)
+
+
+def run_gauge_only(args):
+    """W + K right-moving gauge moves (norm_denorm_going_right_) of a
+    (chi, chi, 2) site into its neighbour, through the Level-0 C-ABI."""
+    import time as _t
+
+    import nutcracker_b200 as nb
+
+    rng = np.random.default_rng(args.seed)
+    chi = args.chi
+    A = np.asfortranarray(rng.standard_normal((chi, chi, 2)) + 1j * rng.standard_normal((chi, chi, 2)))
+    B = np.asfortranarray(rng.standard_normal((chi, chi, 2)) + 1j * rng.standard_normal((chi, chi, 2)))
+    for _ in range(args.warmup):
+        nb.Core.norm_denorm_going_right(chi, chi, chi, 2, 2, A, B)
+    t0 = _t.perf_counter()
+    for _ in range(args.steps):
+        nb.Core.norm_denorm_going_right(chi, chi, chi, 2, 2, A, B)
+    t = (_t.perf_counter() - t0) / args.steps
+    print(json.dumps({"gauge_chi": chi, "ms_with_host_copies": t * 1e3}), flush=True)
 
 
 # ---------------------------------------------------------------------------
@@ -281,7 +305,8 @@ def run_ours(args, rank, world):
             td.barrier()
 
     ops = operators.heisenberg(args.sites)
-    chain = Chain(ops, initial_bandwidth_dimension=args.chi_start, seed=args.seed + 7919 * rank)
+    chain = Chain(ops, initial_bandwidth_dimension=args.chi_start, seed=args.seed + 7919 * rank,
+                  time_phases=1 if args.phases else 0)
     for _ in range(args.presweeps):
         chain.perform_optimization_sweep()
     chain.increase_bandwidth_dimension(args.chi)
@@ -390,7 +415,9 @@ def run_ours(args, rank, world):
                      "gemm_share_of_step": (pms.value / 1e3) / elapsed if elapsed > 0 else None},
         "clocks": clk,
         "chain": {"energy": energy, "energy_per_site": energy / args.sites, "matvecs_per_site": matvecs / max(solves, 1),
-                  "site_solves": solves, "failures": info1["failures"] - info0["failures"]},
+                  "site_solves": solves, "failures": info1["failures"] - info0["failures"],
+                  "phase_seconds": {k: info1["seconds_" + k] - info0["seconds_" + k]
+                                    for k in ("solve", "gauge", "environment", "projector")} if args.phases else None},
     }
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.sites, args.chi)
@@ -411,6 +438,8 @@ def main():
     try:
         if args.heff_only:
             run_heff_only(args)
+        elif args.gauge_only:
+            run_gauge_only(args)
         elif args.impl == "reference":
             run_reference(args, rank)
         else:

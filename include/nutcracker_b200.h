@@ -281,6 +281,7 @@ typedef struct {
     uint32_t krylov_dimension;        /* Lanczos basis size (default 24) */
     uint64_t seed;                    /* random initial states */
     uint32_t strict;                  /* nonzero: a failed site solve is an error */
+    uint32_t time_phases;             /* nonzero: synchronise and time each phase (diagnostics) */
 } nc_chain_options;
 
 /* One MPO site (OperatorSite, tensors.hpp:1641-1854): indices (2,nnz)
@@ -297,6 +298,9 @@ typedef struct {
     uint64_t sweeps, site_solves, matvecs, moves, failures;
     int32_t last_failure;             /* optimizer failure kind, 0 = none */
     double energy;
+    /* seconds spent per phase when time_phases is set: site solves, gauge
+       moves, environment updates, projector matrices */
+    double seconds_solve, seconds_gauge, seconds_environment, seconds_projector;
 } nc_chain_info;
 
 typedef struct nc_chain nc_chain;

@@ -9,6 +9,7 @@
 // (bl,bl,cl), valid for i <= cursor; Renv[i] = environment right of site i
 // (br,br,cr), valid for i >= cursor; likewise Lov/Rov per projector.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -65,6 +66,26 @@ struct ProjSite {
 };
 
 constexpr int kMaxSweeps = 500;
+
+// Diagnostic phase timer: synchronises the stream on entry and exit and adds
+// the wall time to `acc` (only when the chain's time_phases option is set).
+struct PhaseTimer {
+    cudaStream_t s;
+    double* acc;
+    std::chrono::steady_clock::time_point t0;
+    PhaseTimer(bool on, cudaStream_t st, double* a) : s(st), acc(on ? a : nullptr) {
+        if (acc) {
+            cudaStreamSynchronize(s);
+            t0 = std::chrono::steady_clock::now();
+        }
+    }
+    ~PhaseTimer() {
+        if (acc) {
+            cudaStreamSynchronize(s);
+            *acc += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        }
+    }
+};
 
 inline bool outside_tolerance(double a, double b, double tol) {
     // utilities.hpp:418-420
@@ -322,25 +343,38 @@ struct Chain {
         const int c = cur;
         if (dir > 0) {
             NC_ARG(c + 1 < N, "cannot move right from the last site");
-            // site c -> left-normalised, site c+1 absorbs the factor and becomes the centre
-            gauge_right(ctx, bl(c), br(c), br(c + 1), phys[c], phys[c + 1], site[c].p, site[c + 1].p, spare_a.p,
-                        spare_b.p);
-            std::swap(site[c], spare_a);
-            std::swap(site[c + 1], spare_b);
-            normalize(site[c + 1].p, (long long)site_elems(c + 1));
-            absorb_left(c);
+            {
+                // site c -> left-normalised, site c+1 absorbs the factor and becomes the centre
+                PhaseTimer t(opt.time_phases, ctx.stream, &stats.t_gauge);
+                gauge_right(ctx, bl(c), br(c), br(c + 1), phys[c], phys[c + 1], site[c].p, site[c + 1].p,
+                            spare_a.p, spare_b.p);
+                std::swap(site[c], spare_a);
+                std::swap(site[c + 1], spare_b);
+                normalize(site[c + 1].p, (long long)site_elems(c + 1));
+            }
+            {
+                PhaseTimer t(opt.time_phases, ctx.stream, &stats.t_env);
+                absorb_left(c);
+            }
             cur = c + 1;
         } else {
             NC_ARG(c > 0, "cannot move left from the first site");
-            gauge_left(ctx, bl(c - 1), br(c - 1), br(c), phys[c - 1], phys[c], site[c - 1].p, site[c].p, spare_a.p,
-                       spare_b.p);
-            std::swap(site[c - 1], spare_a);
-            std::swap(site[c], spare_b);
-            normalize(site[c - 1].p, (long long)site_elems(c - 1));
-            absorb_right(c);
+            {
+                PhaseTimer t(opt.time_phases, ctx.stream, &stats.t_gauge);
+                gauge_left(ctx, bl(c - 1), br(c - 1), br(c), phys[c - 1], phys[c], site[c - 1].p, site[c].p,
+                           spare_a.p, spare_b.p);
+                std::swap(site[c - 1], spare_a);
+                std::swap(site[c], spare_b);
+                normalize(site[c - 1].p, (long long)site_elems(c - 1));
+            }
+            {
+                PhaseTimer t(opt.time_phases, ctx.stream, &stats.t_env);
+                absorb_right(c);
+            }
             cur = c - 1;
         }
         stats.moves++;
+        PhaseTimer t(opt.time_phases, ctx.stream, &stats.t_proj);
         reset_projector_matrix();
     }
 
@@ -357,6 +391,7 @@ struct Chain {
     }
 
     int optimize_site_once() {
+        PhaseTimer timer(opt.time_phases, ctx.stream, &stats.t_solve);
         const long long n = (long long)site_elems(cur);
         double ev = 0, normal = 0;
         EigenStats es;
@@ -573,6 +608,7 @@ ChainOptions to_options(const nc_chain_options* o) {
     c.krylov_dim = o->krylov_dimension ? (int)o->krylov_dimension : 24;
     c.seed = o->seed;
     c.strict = o->strict != 0;
+    c.time_phases = o->time_phases != 0;
     return c;
 }
 }  // namespace
@@ -680,6 +716,10 @@ int nc_chain_get_info(nc_chain* c, nc_chain_info* info) {
         info->failures = ch.stats.failures;
         info->last_failure = ch.stats.last_failure;
         info->energy = ch.energy;
+        info->seconds_solve = ch.stats.t_solve;
+        info->seconds_gauge = ch.stats.t_gauge;
+        info->seconds_environment = ch.stats.t_env;
+        info->seconds_projector = ch.stats.t_proj;
     })
 }
 

@@ -35,6 +35,7 @@ struct ChainOptions {
     int krylov_dim = 24;
     uint64_t seed = 1;
     bool strict = false;                // raise on a site failure instead of keeping the old site
+    bool time_phases = false;           // synchronise and time each phase
 };
 
 struct OperatorSiteDesc {
@@ -46,6 +47,7 @@ struct OperatorSiteDesc {
 struct ChainStats {
     uint64_t sweeps = 0, site_solves = 0, matvecs = 0, moves = 0, failures = 0;
     int last_failure = 0;
+    double t_solve = 0, t_gauge = 0, t_env = 0, t_proj = 0;
 };
 
 }  // namespace nc

@@ -97,6 +97,10 @@ struct Context {
     size_t pinned_bytes = 0;
     uint64_t launches = 0;   // kernels launched by this library on this context
     int krylov_dim = 24;     // Lanczos basis size before a restart
+    // Workspace arena for GEMM split-K partials and QR scratch: the context
+    // arena, or a captured graph's private arena while it is being recorded.
+    Arena* ws_override = nullptr;
+    Arena& scratch() { return ws_override ? *ws_override : arena; }
     // Kernel timing (nc_profile_begin/end): CUDA events around every complex
     // GEMM of at least profile_min_flops, on the launching stream.
     bool profile = false;

@@ -16,6 +16,8 @@
 // accumulation of the block reflectors (zungqr order).
 #include <algorithm>
 #include <cmath>
+#include <memory>
+#include <vector>
 
 #include "nc_common.cuh"
 #include "nc_kernels.h"
@@ -222,20 +224,24 @@ __global__ void __launch_bounds__(PT) panel_apply_kernel(int mp, int jb, const c
 __global__ void build_t_kernel(int nb, const cplx* __restrict__ G, const cplx* __restrict__ tau,
                                cplx* __restrict__ T, int ldt) {
     // thread k owns row k of T; the diagonal is written by thread 0 and read
-    // by thread k in later columns, after a __syncthreads.
-    const int k = threadIdx.x;
-    for (int i = k; i < ldt * nb; i += blockDim.x) T[i] = cmake(0, 0);
-    __syncthreads();
-    for (int c = 0; c < nb; ++c) {
-        cplx tc = tau[c];
-        if (k < c) {
-            cplx acc = cmake(0, 0);
-            for (int l = k; l < c; ++l) acc = cadd(acc, cmul(T[k + ldt * l], G[l + nb * c]));
-            T[k + ldt * c] = cscale(cmul(tc, acc), -1.0);
-        }
-        if (k == 0) T[c + ldt * c] = tc;
-        __syncthreads();
+    // Uses T^{-1} = striu(V^H V) + diag(1/tau) (the compact-WY identity of
+    // Puglisi 1992 / Joffrain et al. 2006): thread j back-substitutes column
+    // j of T independently, T(i,j) = -tau_i sum_{l=i+1..j} G(i,l) T(l,j),
+    // T(j,j) = tau_j (a zero tau gives a zero row and column, as it should).
+    const int j = threadIdx.x;
+    if (j >= nb) return;
+    cplx col[NB];
+    for (int i = 0; i < nb; ++i) col[i] = cmake(0, 0);
+    col[j] = tau[j];
+    for (int i = j - 1; i >= 0; --i) {
+        cplx acc = cmake(0, 0);
+        for (int l = i + 1; l <= j; ++l) acc = cadd(acc, cmul(G[i + nb * l], col[l]));
+        col[i] = cscale(cmul(tau[i], acc), -1.0);
     }
+    for (int i = 0; i < NB; ++i) T[i + (long long)ldt * j] = (i < nb) ? col[i] : cmake(0, 0);
+    if (j == 0)
+        for (int c = nb; c < NB; ++c)
+            for (int i = 0; i < NB; ++i) T[i + (long long)ldt * c] = cmake(0, 0);
 }
 
 __global__ void identity_cols(long long m, int n, cplx* __restrict__ Q) {
@@ -278,16 +284,17 @@ void launch_panel(Context& ctx, int mp, int jb, cplx* A, long long lda, cplx* V,
 void householder_qr(Context& ctx, int m, int n, cplx* A, cplx* Q, cplx* R, bool conjR) {
     NC_ARG(m >= n && n >= 1, "householder_qr: need m >= n >= 1");
     NC_ARG(m <= PT * PMAXROWS, "householder_qr: at most 2048 rows (bond x physical dimension)");
-    ArenaFrame f(ctx.arena);
+    Arena& ar = ctx.scratch();
+    ArenaFrame f(ar);
     const long long lda = m;
-    cplx* V = ctx.arena.alloc_n<cplx>((size_t)m * n);
-    cplx* tau = ctx.arena.alloc_n<cplx>(n);
+    cplx* V = ar.alloc_n<cplx>((size_t)m * n);
+    cplx* tau = ar.alloc_n<cplx>(n);
     const int nblocks = (n + NB - 1) / NB;
-    cplx* Tb = ctx.arena.alloc_n<cplx>((size_t)nblocks * NB * NB);
-    cplx* T4 = ctx.arena.alloc_n<cplx>(JB * JB);
-    cplx* G = ctx.arena.alloc_n<cplx>(NB * NB);
-    cplx* W = ctx.arena.alloc_n<cplx>((size_t)NB * n);
-    cplx* W2 = ctx.arena.alloc_n<cplx>((size_t)NB * n);
+    cplx* Tb = ar.alloc_n<cplx>((size_t)nblocks * NB * NB);
+    cplx* T4 = ar.alloc_n<cplx>(JB * JB);
+    cplx* G = ar.alloc_n<cplx>(NB * NB);
+    cplx* W = ar.alloc_n<cplx>((size_t)NB * n);
+    cplx* W2 = ar.alloc_n<cplx>((size_t)NB * n);
     zfill(ctx, (long long)m * n, cmake(0, 0), V);
 
     for (int ob = 0; ob < nblocks; ++ob) {
@@ -357,21 +364,90 @@ void householder_qr(Context& ctx, int m, int n, cplx* A, cplx* Q, cplx* R, bool 
 // gauge moves (core.f95:2708-2960 semantics, QR gauge)
 // ---------------------------------------------------------------------------
 
+// A QR of one shape recorded as a CUDA graph: a gauge move issues a few
+// hundred short kernels (the panels are latency bound), so replaying a
+// pre-recorded graph removes the per-launch host overhead.  The plan owns its
+// input/output buffers and a private workspace arena, so the pointers baked
+// into the graph stay valid and are never shared with other work.
+struct QrPlan {
+    int m = 0, n = 0;
+    bool conjR = false;
+    Arena arena;
+    cplx* X = nullptr;   // input (m x n), overwritten
+    cplx* Q = nullptr;   // explicit Q (m x n)
+    cplx* R = nullptr;   // R (n x n), conjugated if conjR
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t kernels = 0;
+    ~QrPlan() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+};
+
+namespace {
+QrPlan& qr_plan(Context& ctx, int m, int n, bool conjR) {
+    thread_local std::vector<std::unique_ptr<QrPlan>> plans;
+    for (auto& p : plans)
+        if (p->m == m && p->n == n && p->conjR == conjR) return *p;
+    auto p = std::make_unique<QrPlan>();
+    p->m = m; p->n = n; p->conjR = conjR;
+    p->X = p->arena.alloc_n<cplx>((size_t)m * n);
+    p->Q = p->arena.alloc_n<cplx>((size_t)m * n);
+    p->R = p->arena.alloc_n<cplx>((size_t)n * n);
+    plans.push_back(std::move(p));
+    return *plans.back();
+}
+
+// Run the QR of plan.X; the first run of a shape executes directly (so the
+// private arena grows to its final size) and then records the graph.
+void qr_run(Context& ctx, QrPlan& P) {
+    if (P.exec) {
+        NC_CUDA(cudaGraphLaunch(P.exec, ctx.stream));
+        ctx.launches += P.kernels;
+        return;
+    }
+    const bool prof = ctx.profile;
+    ctx.profile = false;
+    ctx.ws_override = &P.arena;
+    try {
+        householder_qr(ctx, P.m, P.n, P.X, P.Q, P.R, P.conjR);
+        const uint64_t l0 = ctx.launches;
+        NC_CUDA(cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeRelaxed));
+        try {
+            householder_qr(ctx, P.m, P.n, P.X, P.Q, P.R, P.conjR);
+        } catch (...) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(ctx.stream, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        NC_CUDA(cudaStreamEndCapture(ctx.stream, &P.graph));
+        P.kernels = ctx.launches - l0;
+        ctx.launches = l0;
+        NC_CUDA(cudaGraphInstantiate(&P.exec, P.graph, 0));
+    } catch (...) {
+        ctx.ws_override = nullptr;
+        ctx.profile = prof;
+        throw;
+    }
+    ctx.ws_override = nullptr;
+    ctx.profile = prof;
+}
+}  // namespace
+
 void gauge_right(Context& ctx, int bl, int bm, int br, int dl, int dr, const cplx* A, const cplx* B,
                  cplx* normA, cplx* denormB) {
     const int K = bl * dl;
     NC_ARG(K >= bm, "not enough degrees of freedom to normalize");
-    ArenaFrame f(ctx.arena);
-    cplx* X = ctx.arena.alloc_n<cplx>((size_t)K * bm);
-    cplx* Qt = ctx.arena.alloc_n<cplx>((size_t)K * bm);
-    cplx* Rt = ctx.arena.alloc_n<cplx>((size_t)bm * bm);
+    QrPlan& P = qr_plan(ctx, K, bm, false);
     const int p_t[3] = {1, 0, 2};
-    permute3(ctx, A, bm, K, 1, p_t, true, X);               // X = A^H  (K x bm)
-    householder_qr(ctx, K, bm, X, Qt, Rt, false);            // A^H = Qt Rt
-    permute3(ctx, Qt, K, bm, 1, p_t, true, normA);           // normA = Qt^H
+    permute3(ctx, A, bm, K, 1, p_t, true, P.X);             // X = A^H  (K x bm)
+    qr_run(ctx, P);                                          // A^H = Qt Rt
+    permute3(ctx, P.Q, K, bm, 1, p_t, true, normA);         // normA = Qt^H
     if (B && denormB) {
         // denormB_s = B_s Rt^H  (neighbour absorbs P = Rt^H on its left index)
-        ZGemmParams p = zgemm_params(OP_N, OP_C, br, bm, bm, B, br, Rt, bm, denormB, br);
+        ZGemmParams p = zgemm_params(OP_N, OP_C, br, bm, bm, B, br, P.R, bm, denormB, br);
         p.batch = dr;
         p.sA0 = (long long)br * bm; p.sB0 = 0; p.sC0 = (long long)br * bm;
         zgemm(p, ctx);
@@ -382,14 +458,12 @@ void gauge_left(Context& ctx, int bl, int bm, int br, int dl, int dr, const cplx
                 cplx* denormA, cplx* normB) {
     const int K = br * dr;
     NC_ARG(K >= bm, "not enough degrees of freedom to normalize");
-    ArenaFrame f(ctx.arena);
-    cplx* X = ctx.arena.alloc_n<cplx>((size_t)K * bm);
-    cplx* Qt = ctx.arena.alloc_n<cplx>((size_t)K * bm);
-    cplx* Rc = ctx.arena.alloc_n<cplx>((size_t)bm * bm);
+    QrPlan& P = qr_plan(ctx, K, bm, true);
+    const cplx* Rc = P.R;
     const int p_rs[3] = {0, 2, 1};
-    permute3(ctx, B, br, bm, dr, p_rs, true, X);             // X((r,s),m) = conj(B(r,m,s))
-    householder_qr(ctx, K, bm, X, Qt, Rc, true);             // Rc = conj(Rt)
-    permute3(ctx, Qt, br, dr, bm, p_rs, true, normB);        // normB(r,m,s) = conj(Qt((r,s),m))
+    permute3(ctx, B, br, bm, dr, p_rs, true, P.X);           // X((r,s),m) = conj(B(r,m,s))
+    qr_run(ctx, P);                                          // Rc = conj(Rt)
+    permute3(ctx, P.Q, br, dr, bm, p_rs, true, normB);       // normB(r,m,s) = conj(Qt((r,s),m))
     if (A && denormA) {
         // denormA = conj(Rt) * A  (as bm x bl*dl)
         zgemm(zgemm_params(OP_N, OP_N, bm, bl * dl, bm, Rc, bm, A, bm, denormA, bm), ctx);

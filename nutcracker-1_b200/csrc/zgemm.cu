@@ -283,9 +283,9 @@ void zgemm_ctx(const ZGemmParams& p_in, Context& ctx) {
     }
     int kchunk = (int)(((p.K + nsplit - 1) / nsplit + 15) / 16 * 16);
     nsplit = (p.K + kchunk - 1) / kchunk;
-    ArenaFrame f(ctx.arena);
+    ArenaFrame f(ctx.scratch());
     const long long mn = (long long)p.M * p.N;
-    cplx* ws = ctx.arena.alloc_n<cplx>((size_t)mn * p.batch * nsplit);
+    cplx* ws = ctx.scratch().alloc_n<cplx>((size_t)mn * p.batch * nsplit);
     ZGemmParams q = p;
     q.kchunk = kchunk;
     q.nsplit = nsplit;

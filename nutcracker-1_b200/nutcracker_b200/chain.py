@@ -27,6 +27,7 @@ class nc_chain_options(ct.Structure):
         ("krylov_dimension", ct.c_uint32),
         ("seed", ct.c_uint64),
         ("strict", ct.c_uint32),
+        ("time_phases", ct.c_uint32),
     ]
 
 
@@ -55,6 +56,10 @@ class nc_chain_info(ct.Structure):
         ("failures", ct.c_uint64),
         ("last_failure", ct.c_int32),
         ("energy", ct.c_double),
+        ("seconds_solve", ct.c_double),
+        ("seconds_gauge", ct.c_double),
+        ("seconds_environment", ct.c_double),
+        ("seconds_projector", ct.c_double),
     ]
 
 
