@@ -10,19 +10,24 @@
 //
 // QR layout: right-looking blocked Householder, outer blocks of NB=64 columns
 // (trailing update = three complex GEMMs through the compact WY form
-// I - V T V^H), inner panels of JB=4 columns factorised by one CTA with the
-// panel held in registers (mp <= 2048 rows) and updated inside the outer
-// block by a per-column kernel.  Q is formed explicitly by backward
-// accumulation of the block reflectors (zungqr order).
+// I - V T V^H).  Each block is factorised by one thread-block cluster of up
+// to 16 CTAs with the block held in registers (mp <= 2048 rows); devices
+// that cannot co-schedule such a cluster use inner panels of JB=4 columns
+// (one CTA each) and a per-column update kernel.  Q is formed explicitly by
+// backward accumulation of the block reflectors (zungqr order).
 #include <algorithm>
 #include <cmath>
 #include <memory>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "nc_common.cuh"
 #include "nc_kernels.h"
 
 namespace nc {
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -220,28 +225,287 @@ __global__ void __launch_bounds__(PT) panel_apply_kernel(int mp, int jb, const c
     }
 }
 
-// Compact-WY T (nb x nb) from G = V^H V (nb x nb) and tau, one CTA.
-__global__ void build_t_kernel(int nb, const cplx* __restrict__ G, const cplx* __restrict__ tau,
-                               cplx* __restrict__ T, int ldt) {
-    // thread k owns row k of T; the diagonal is written by thread 0 and read
-    // Uses T^{-1} = striu(V^H V) + diag(1/tau) (the compact-WY identity of
-    // Puglisi 1992 / Joffrain et al. 2006): thread j back-substitutes column
-    // j of T independently, T(i,j) = -tau_i sum_{l=i+1..j} G(i,l) T(l,j),
-    // T(j,j) = tau_j (a zero tau gives a zero row and column, as it should).
-    const int j = threadIdx.x;
-    if (j >= nb) return;
-    cplx col[NB];
-    for (int i = 0; i < nb; ++i) col[i] = cmake(0, 0);
-    col[j] = tau[j];
-    for (int i = j - 1; i >= 0; --i) {
-        cplx acc = cmake(0, 0);
-        for (int l = i + 1; l <= j; ++l) acc = cadd(acc, cmul(G[i + nb * l], col[l]));
-        col[i] = cscale(cmul(tau[i], acc), -1.0);
+// Compact-WY T (nb x nb, zlarft forward/columnwise) from the strict upper
+// part of G = V^H V and tau:  T(j,j) = tau_j,
+// T(0:j,j) = -tau_j T(0:j,0:j) G(0:j,j).
+// One CTA; row i of T is owned by a quad of lanes (lane q holds T(i,l) for
+// l = q mod 4 in registers), so the columns are produced without any block
+// barrier: each step is a <= 16-term dot per lane and a quad reduction.
+__global__ void __launch_bounds__(4 * NB) build_t_kernel(int nb, const cplx* __restrict__ G,
+                                                        const cplx* __restrict__ tau, cplx* __restrict__ T,
+                                                        int ldt) {
+    __shared__ cplx Gp[NB * (NB - 1) / 2];   // column j at j(j-1)/2, rows 0..j-1
+    __shared__ cplx taus[NB];
+    for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+        const int l = e % nb, j = e / nb;
+        if (l < j) Gp[j * (j - 1) / 2 + l] = G[e];
     }
-    for (int i = 0; i < NB; ++i) T[i + (long long)ldt * j] = (i < nb) ? col[i] : cmake(0, 0);
-    if (j == 0)
-        for (int c = nb; c < NB; ++c)
-            for (int i = 0; i < NB; ++i) T[i + (long long)ldt * c] = cmake(0, 0);
+    for (int e = threadIdx.x; e < NB; e += blockDim.x) taus[e] = (e < nb) ? tau[e] : cmake(0, 0);
+    __syncthreads();
+    const int i = threadIdx.x >> 2, q = threadIdx.x & 3;
+    cplx t[NB / 4];
+#pragma unroll
+    for (int m = 0; m < NB / 4; ++m) t[m] = cmake(0, 0);
+#pragma unroll
+    for (int jm = 0; jm < NB / 4; ++jm) {
+#pragma unroll
+        for (int jq = 0; jq < 4; ++jq) {
+            const int j = 4 * jm + jq;
+            if (j >= nb) break;
+            // partial sum over l = q + 4m, i <= l < j
+            double sr = 0, si = 0;
+#pragma unroll
+            for (int m = 0; m <= jm; ++m) {
+                const int l = q + 4 * m;
+                if (l < j && l >= i) {
+                    const cplx gv = Gp[j * (j - 1) / 2 + l];
+                    sr = fma(t[m].x, gv.x, fma(-t[m].y, gv.y, sr));
+                    si = fma(t[m].x, gv.y, fma(t[m].y, gv.x, si));
+                }
+            }
+            sr += __shfl_xor_sync(0xffffffffu, sr, 1);
+            si += __shfl_xor_sync(0xffffffffu, si, 1);
+            sr += __shfl_xor_sync(0xffffffffu, sr, 2);
+            si += __shfl_xor_sync(0xffffffffu, si, 2);
+            const cplx tj = taus[j];
+            cplx v = cmake(0, 0);
+            if (i < j) v = cscale(cmul(tj, cmake(sr, si)), -1.0);
+            else if (i == j) v = tj;
+            if (q == jq) t[jm] = v;
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < NB / 4; ++m) {
+        const int l = q + 4 * m;
+        T[i + (long long)ldt * l] = (i < nb && l < nb) ? t[m] : cmake(0, 0);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// One outer block (mp x nb, nb <= NB) factorised by a thread-block cluster.
+//
+// The rows are split over the C CTAs of one cluster (at most CQ_MAXR rows
+// each, held in registers: thread (k, g) owns column k at rows g + 8i), so
+// the whole block needs one launch instead of NB/JB panel and update
+// launches.  Column j needs a single cluster-wide reduction: every CTA forms,
+// over its rows below the diagonal,
+//   s_k = sum_r conj(x_r) P(r,k)   for all k   (x = column j)
+// which gives the column norm (k = j), the reflector products with the
+// trailing columns (k > j: w_k = P(j,k) + conj(scale) s_k) and the Gram
+// column of the compact-WY T (k < j: G(k,j) = conj(V(j,k)) + scale conj(s_k)),
+// because v = e_j + scale * x.  Each CTA stores its partial sums (and CTA 0,
+// which holds the pivot rows, row j) into every CTA's shared memory (DSMEM,
+// double-buffered by column parity) and one cluster barrier publishes them;
+// each CTA then reduces the C partials with the same tree, so all CTAs
+// derive bit-identical reflectors.  Reflector tails stay unscaled; the scale
+// of column k is applied on use and at write-back.  The only waits are the
+// hardware block and cluster barriers.
+// ---------------------------------------------------------------------------
+constexpr int CQ_T = 512;             // threads per CTA
+constexpr int CQ_G = CQ_T / NB;       // lanes per column (row interleave)
+constexpr int CQ_MAXC = 16;           // CTAs per cluster (non-portable size)
+constexpr int CQ_MAXR = 128;          // rows per CTA -> mp <= 2048
+constexpr int CQ_RPT = CQ_MAXR / CQ_G;  // rows per thread
+__global__ void __launch_bounds__(CQ_T, 1)
+cluster_block_qr_kernel(int mp, int nb, int rows_per_cta, cplx* __restrict__ A, long long lda,
+                        cplx* __restrict__ V, long long ldv, cplx* __restrict__ tau_out,
+                        cplx* __restrict__ G) {
+    __shared__ cplx recv[2][CQ_MAXC][NB];   // partial sums by source CTA, per column parity
+    __shared__ cplx piv[2][NB];             // pivot row as received, per column parity
+    __shared__ cplx pivst[2][NB];           // pivot row staged by its owners (CTA 0)
+    __shared__ cplx xs[2][CQ_MAXR];         // column j of this CTA's rows
+    __shared__ cplx colscale[NB];
+    __shared__ cplx taus[NB];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int C = (int)cluster.num_blocks();
+    const int rank = (int)cluster.block_rank();
+    const int tid = threadIdx.x, k = tid / CQ_G, g = tid % CQ_G;
+    const int row0 = rank * rows_per_cta;
+    const int nr = max(0, min(rows_per_cta, mp - row0));
+    // Row j (< nb) always lies in CTA 0: rows_per_cta >= nb whenever C > 1
+    // (mp > CQ_MAXR (C-1)), and mp >= nb when C == 1.
+    const bool top = (rank == 0);
+
+    cplx a[CQ_RPT];
+#pragma unroll
+    for (int i = 0; i < CQ_RPT; ++i) {
+        const int r = g + CQ_G * i;
+        a[i] = (r < nr && k < nb) ? A[(row0 + r) + (long long)k * lda] : cmake(0, 0);
+    }
+    if (k == 0) {
+#pragma unroll
+        for (int i = 0; i < CQ_RPT; ++i) xs[0][g + CQ_G * i] = a[i];
+    }
+    if (top && g == 0) pivst[0][k] = a[0];   // row 0
+    cluster.sync();
+
+    for (int j = 0; j < nb; ++j) {
+        const int p = j & 1;
+        // phase 1: partial sums over this CTA's rows below the diagonal.  Only
+        // CTA 0's first NB rows can lie on or above the diagonal (j < NB).
+        double s0r = 0, s0i = 0, s1r = 0, s1i = 0;
+#pragma unroll
+        for (int i = 0; i < CQ_RPT; i += 2) {
+            const int r0 = g + CQ_G * i, r1 = r0 + CQ_G;
+            const cplx x0 = xs[p][r0], x1 = xs[p][r1];
+            const bool u0 = !top || r0 >= NB || r0 > j, u1 = !top || r1 >= NB || r1 > j;
+            if (u0) {
+                s0r = fma(x0.x, a[i].x, fma(x0.y, a[i].y, s0r));
+                s0i = fma(x0.x, a[i].y, fma(-x0.y, a[i].x, s0i));
+            }
+            if (u1) {
+                s1r = fma(x1.x, a[i + 1].x, fma(x1.y, a[i + 1].y, s1r));
+                s1i = fma(x1.x, a[i + 1].y, fma(-x1.y, a[i + 1].x, s1i));
+            }
+        }
+        double sr = s0r + s1r, si = s0i + s1i;
+#pragma unroll
+        for (int o = 1; o < CQ_G; o <<= 1) {
+            sr += __shfl_xor_sync(0xffffffffu, sr, o);
+            si += __shfl_xor_sync(0xffffffffu, si, o);
+        }
+        cplx part = cmake(sr, si);
+        cplx pv = cmake(0, 0);
+        if (k < j) part = cmul(part, colscale[k]);
+        if (top) {
+            pv = pivst[p][k];
+            if (k < j) pv = cmul(pv, colscale[k]);
+        }
+        // phase 2: push to every CTA of the cluster (DSMEM stores), then one
+        // cluster barrier (release/acquire) publishes them
+        for (int d = g; d < C; d += CQ_G) {
+            cluster.map_shared_rank(&recv[p][rank][0], d)[k] = part;
+            if (top) cluster.map_shared_rank(&piv[p][0], d)[k] = pv;
+        }
+        cluster.sync();
+        // phase 3: the CQ_G lanes of column k split the sources; a fixed
+        // reduction tree keeps every CTA bit-identical
+        cplx Sk = cmake(0, 0), Sj = cmake(0, 0);
+        for (int c = g; c < C; c += CQ_G) {
+            Sk = cadd(Sk, recv[p][c][k]);
+            Sj = cadd(Sj, recv[p][c][j]);
+        }
+#pragma unroll
+        for (int o = 1; o < CQ_G; o <<= 1) {
+            Sk.x += __shfl_xor_sync(0xffffffffu, Sk.x, o);
+            Sk.y += __shfl_xor_sync(0xffffffffu, Sk.y, o);
+            Sj.x += __shfl_xor_sync(0xffffffffu, Sj.x, o);
+        }
+        const double xnorm2 = Sj.x;
+        const cplx alpha = piv[p][j];
+        const cplx pk = piv[p][k];
+        cplx t = cmake(0, 0), scale = cmake(1, 0), diag = alpha;
+        const bool reflect = !(xnorm2 == 0.0 && alpha.y == 0.0);
+        if (reflect) {
+            const double beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xnorm2), alpha.x);
+            const cplx den = cmake(alpha.x - beta, alpha.y);
+            const double ib = 1.0 / beta;
+            const double idd = 1.0 / (den.x * den.x + den.y * den.y);
+            t = cmake((beta - alpha.x) * ib, -alpha.y * ib);
+            scale = cmake(den.x * idd, -den.y * idd);
+            diag = cmake(beta, 0);
+        }
+        if (tid == 0) {
+            colscale[j] = scale;
+            taus[j] = t;
+        }
+        if (top && g == 0 && k < j) G[k + (long long)nb * j] = cadd(cconj(pk), cmul(scale, cconj(Sk)));
+        // phase 4: apply H_j^H = I - conj(tau) v v^H to the trailing columns
+        if (reflect && k > j && k < nb) {
+            const cplx cf = cmul(cconj(t), cadd(pk, cmul(cconj(scale), Sk)));
+            const cplx ef = cmul(scale, cf);
+            if (top) {
+#pragma unroll
+                for (int i = 0; i < CQ_RPT; ++i) {
+                    const int r = g + CQ_G * i;
+                    if (r < NB && r == j) a[i] = csub(a[i], cf);
+                    else if (r >= NB || r > j) a[i] = csub(a[i], cmul(xs[p][r], ef));
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < CQ_RPT; ++i) a[i] = csub(a[i], cmul(xs[p][g + CQ_G * i], ef));
+            }
+        }
+        if (top) {
+            // diagonal of R, and stage row j+1 for the next pivot broadcast
+#pragma unroll
+            for (int i = 0; i < CQ_RPT / 2; ++i) {   // rows < NB
+                const int r = g + CQ_G * i;
+                if (k == j && r == j) a[i] = diag;
+                if (r == j + 1) pivst[p ^ 1][k] = a[i];
+            }
+        }
+        if (k == j + 1) {
+#pragma unroll
+            for (int i = 0; i < CQ_RPT; ++i) xs[p ^ 1][g + CQ_G * i] = a[i];
+        }
+        __syncthreads();
+    }
+
+    {
+#pragma unroll
+        for (int i = 0; i < CQ_RPT; ++i) {
+            const int r = g + CQ_G * i, prow = row0 + r;
+            if (r < nr && k < nb) {
+                cplx v = a[i];
+                if (prow > k) v = cmul(v, colscale[k]);
+                A[prow + (long long)k * lda] = v;
+                V[prow + (long long)k * ldv] = (prow > k) ? v : cmake(prow == k ? 1.0 : 0.0, 0);
+            }
+        }
+        if (rank == 0)
+            for (int c = tid; c < nb; c += CQ_T) tau_out[c] = taus[c];
+    }
+    cluster.sync();   // no CTA leaves while another may still write its shared memory
+}
+
+// Cluster launch support (size CQ_MAXC needs the non-portable opt-in); a
+// device that cannot co-schedule the cluster uses the per-panel path.
+bool cluster_qr_available() {
+    static int state = -1;
+    if (state >= 0) return state == 1;
+    state = 0;
+    if (cudaFuncSetAttribute(cluster_block_qr_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(CQ_MAXC);
+    cfg.blockDim = dim3(CQ_T);
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = CQ_MAXC;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, cluster_block_qr_kernel, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    state = nclusters >= 1 ? 1 : 0;
+    return state == 1;
+}
+
+void launch_cluster_block(Context& ctx, int mp, int nb, cplx* A, long long lda, cplx* V, long long ldv,
+                          cplx* tau, cplx* G) {
+    const int C = std::max(1, std::min(CQ_MAXC, (mp + CQ_MAXR - 1) / CQ_MAXR));
+    const int rows = (mp + C - 1) / C;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(C);
+    cfg.blockDim = dim3(CQ_T);
+    cfg.stream = ctx.stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    NC_CUDA(cudaLaunchKernelEx(&cfg, cluster_block_qr_kernel, mp, nb, rows, A, lda, V, ldv, tau, G));
+    ctx.launches++;
 }
 
 __global__ void identity_cols(long long m, int n, cplx* __restrict__ Q) {
@@ -295,29 +559,33 @@ void householder_qr(Context& ctx, int m, int n, cplx* A, cplx* Q, cplx* R, bool 
     cplx* G = ar.alloc_n<cplx>(NB * NB);
     cplx* W = ar.alloc_n<cplx>((size_t)NB * n);
     cplx* W2 = ar.alloc_n<cplx>((size_t)NB * n);
-    zfill(ctx, (long long)m * n, cmake(0, 0), V);
-
+    const bool use_cluster = cluster_qr_available();
+    if (!use_cluster) zfill(ctx, (long long)m * n, cmake(0, 0), V);
     for (int ob = 0; ob < nblocks; ++ob) {
         const int j0 = ob * NB;
         const int nb = std::min(NB, n - j0);
         const int mp = m - j0;
-        // inner panels
-        for (int jj = j0; jj < j0 + nb; jj += JB) {
-            const int jb = std::min(JB, j0 + nb - jj);
-            launch_panel(ctx, m - jj, jb, A + jj + jj * lda, lda, V + jj + jj * (long long)m, m, tau + jj, T4);
-            const int rest = j0 + nb - (jj + jb);
-            if (rest > 0) {
-                panel_apply_kernel<<<rest, PT, 0, ctx.stream>>>(m - jj, jb, V + jj + jj * (long long)m, m, T4,
-                                                                A + jj + (jj + jb) * lda, lda);
-                NC_CHECK_LAUNCH();
-                ctx.launches++;
-            }
-        }
-        // compact WY T for the outer block
         const cplx* Vb = V + j0 + j0 * (long long)m;
-        zgemm(zgemm_params(OP_C, OP_N, nb, nb, mp, Vb, m, Vb, m, G, nb), ctx);
         cplx* T = Tb + (size_t)ob * NB * NB;
-        build_t_kernel<<<1, NB, 0, ctx.stream>>>(nb, G, tau + j0, T, NB);
+        if (use_cluster) {
+            launch_cluster_block(ctx, mp, nb, A + j0 + j0 * lda, lda, V + j0 + j0 * (long long)m, m, tau + j0, G);
+        } else {
+            for (int jj = j0; jj < j0 + nb; jj += JB) {
+                const int jb = std::min(JB, j0 + nb - jj);
+                launch_panel(ctx, m - jj, jb, A + jj + jj * lda, lda, V + jj + jj * (long long)m, m, tau + jj,
+                             T4);
+                const int rest = j0 + nb - (jj + jb);
+                if (rest > 0) {
+                    panel_apply_kernel<<<rest, PT, 0, ctx.stream>>>(m - jj, jb, V + jj + jj * (long long)m, m,
+                                                                    T4, A + jj + (jj + jb) * lda, lda);
+                    NC_CHECK_LAUNCH();
+                    ctx.launches++;
+                }
+            }
+            zgemm(zgemm_params(OP_C, OP_N, nb, nb, mp, Vb, m, Vb, m, G, nb), ctx);
+        }
+        // compact WY T for the outer block from G = V^H V (strict upper part)
+        build_t_kernel<<<1, 4 * NB, 0, ctx.stream>>>(nb, G, tau + j0, T, NB);
         NC_CHECK_LAUNCH();
         ctx.launches++;
         // trailing update: A2 -= V T^H (V^H A2)
