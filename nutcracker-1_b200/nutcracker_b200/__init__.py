@@ -22,7 +22,7 @@ LIB_PATH = os.path.join(_PKG, "lib", "libnutcracker_b200.so")
 
 if not os.path.exists(LIB_PATH):
     raise ImportError("nutcracker_b200: CUDA library not built (%s); run "
-                      "`python -m nutcracker_b200.build` in nutcracker-1_b200/" % LIB_PATH)
+                      "`python nutcracker-1_b200/nutcracker_b200/build.py`" % LIB_PATH)
 
 lib = ct.CDLL(LIB_PATH)
 

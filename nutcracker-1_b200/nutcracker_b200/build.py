@@ -1,6 +1,9 @@
 """Build the sm_100a shared library in-tree.
 
-    python -m nutcracker_b200.build        (from nutcracker-1_b200/)
+    python nutcracker-1_b200/nutcracker_b200/build.py [--force]
+
+(run as a script or loaded by path: importing the ``nutcracker_b200``
+package requires the library this script produces).
 
 Compiles every ``csrc/*.cu`` with
 ``nvcc -gencode arch=compute_100a,code=sm_100a -O3 -lineinfo`` and links
