@@ -47,9 +47,14 @@ int nc_synchronize(void);
 /* Start timing every complex GEMM of at least `min_flops` algorithmic flops
    with CUDA events on this thread's stream. */
 int nc_profile_begin(double min_flops);
-/* Stop timing; report the number of timed GEMMs, their summed device time
-   (ms) and summed algorithmic flops (8*M*N*K per complex product). */
+/* Stop timing; report the number of timed FP64 complex GEMMs, their summed
+   device time (ms) and summed algorithmic flops (8*M*N*K per complex
+   product). */
 int nc_profile_end(uint64_t* launches, double* total_ms, double* total_flops);
+/* Without stopping: the same totals for one kind of timed GEMM, kind 0 =
+   FP64 complex GEMM, kind 1 = tcgen05 3xTF32 GEMM (flops counted as the
+   TF32 tensor work, 2*M*Nr*Kr per segment, three segments per product). */
+int nc_profile_query(int kind, uint64_t* launches, double* total_ms, double* total_flops);
 
 /* Device-pointer effective-Hamiltonian product y = H_eff x for one site
    (the strategy-3 `operate_on` of core.f95:2529-2556 without projectors):
@@ -59,6 +64,23 @@ int nc_profile_end(uint64_t* launches, double* total_ms, double* total_flops);
 int nc_heff_apply_dev(uint32_t bl, uint32_t br, uint32_t cl, uint32_t cr, uint32_t d, uint32_t nnz,
                       const uint32_t* idx_dev, const void* W_dev, const void* L_dev,
                       const void* R_dev, const void* x_dev, void* y_dev);
+
+/* Precision form of nc_heff_apply_dev: the two complex contractions run on
+   the tcgen05 tensor cores in 3xTF32 (each operand split into two TF32
+   halves, three products, FP32 accumulation); the input, output and the
+   sparse-MPO mix stay FP64.  Relative error ~1e-6 of |H_eff x|.  Device
+   pointers as for nc_heff_apply_dev; synchronises this thread's stream
+   before returning.  Returns a status code. */
+int nc_heff_apply_mixed_dev(uint32_t bl, uint32_t br, uint32_t cl, uint32_t cr, uint32_t d, uint32_t nnz,
+                            const uint32_t* idx_dev, const void* W_dev, const void* L_dev,
+                            const void* R_dev, const void* x_dev, void* y_dev);
+
+/* C = A B for column-major complex128 device matrices A (M x K), B (K x N),
+   C (M x N) on the tcgen05 tensor cores: 3xTF32 when `three` is nonzero,
+   else one TF32 product.  The GEMM under the precision form, exposed for
+   testing; synchronises this thread's stream.  Returns a status code. */
+int nc_tc_zgemm_dev(uint32_t M, uint32_t N, uint32_t K, const void* A_dev, const void* B_dev,
+                    void* C_dev, int three);
 
 /* No counterpart in the reference.  The same H_eff product as
    nc_heff_apply_dev for callers that cannot let the library allocate

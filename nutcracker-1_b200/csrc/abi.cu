@@ -137,17 +137,41 @@ int nc_profile_end(uint64_t* launches, double* total_ms, double* total_flops) {
     Context& ctx = Context::get();
     NC_CUDA(cudaStreamSynchronize(ctx.stream));
     double ms = 0, fl = 0;
+    uint64_t n = 0;
     for (size_t i = 0; i < ctx.prof_used; ++i) {
+        if (ctx.prof_kind[i] != 0) continue;
+        ++n;
         float t = 0;
         NC_CUDA(cudaEventElapsedTime(&t, ctx.prof_start[i], ctx.prof_stop[i]));
         ms += t;
         fl += ctx.prof_flops[i];
     }
-    *launches = ctx.prof_used;
+    *launches = n;
     *total_ms = ms;
     *total_flops = fl;
     ctx.profile = false;
     ctx.prof_used = 0;
+    NC_ABI_END
+    return g_status;
+}
+
+int nc_profile_query(int kind, uint64_t* launches, double* total_ms, double* total_flops) {
+    NC_ABI_BEGIN
+    Context& ctx = Context::get();
+    NC_CUDA(cudaStreamSynchronize(ctx.stream));
+    double ms = 0, fl = 0;
+    uint64_t n = 0;
+    for (size_t i = 0; i < ctx.prof_used; ++i) {
+        if (ctx.prof_kind[i] != kind) continue;
+        ++n;
+        float t = 0;
+        NC_CUDA(cudaEventElapsedTime(&t, ctx.prof_start[i], ctx.prof_stop[i]));
+        ms += t;
+        fl += ctx.prof_flops[i];
+    }
+    *launches = n;
+    *total_ms = ms;
+    *total_flops = fl;
     NC_ABI_END
     return g_status;
 }
@@ -170,6 +194,33 @@ int nc_heff_apply_dev(uint32_t bl, uint32_t br, uint32_t cl, uint32_t cr, uint32
     ArenaFrame f(ctx.arena);
     cplx* ws = ctx.arena.alloc_n<cplx>(heff_workspace_elems(bl, br, op));
     heff_apply(ctx, bl, br, op, (const cplx*)L_dev, (const cplx*)R_dev, (const cplx*)x_dev, (cplx*)y_dev, ws);
+    NC_ABI_END
+    return g_status;
+}
+
+int nc_heff_apply_mixed_dev(uint32_t bl, uint32_t br, uint32_t cl, uint32_t cr, uint32_t d, uint32_t nnz,
+                            const uint32_t* idx_dev, const void* W_dev, const void* L_dev, const void* R_dev,
+                            const void* x_dev, void* y_dev) {
+    NC_ABI_BEGIN
+    Context& ctx = Context::get();
+    MpoSite op;
+    op.d = (int)d; op.cl = (int)cl; op.cr = (int)cr; op.nnz = (int)nnz;
+    op.idx = idx_dev; op.W = (const cplx*)W_dev;
+    ArenaFrame f(ctx.arena);
+    float* buf = ctx.arena.alloc_n<float>(mixed_heff_floats(bl, br, op));
+    MixedHeff h;
+    mixed_heff_prepare(ctx, bl, br, op, (const cplx*)L_dev, (const cplx*)R_dev, buf, &h);
+    heff_apply_mixed(ctx, h, (const cplx*)x_dev, (cplx*)y_dev);
+    tc_check(ctx);
+    NC_ABI_END
+    return g_status;
+}
+
+int nc_tc_zgemm_dev(uint32_t M, uint32_t N, uint32_t K, const void* A_dev, const void* B_dev, void* C_dev,
+                    int three) {
+    NC_ABI_BEGIN
+    tc_zgemm(Context::get(), (int)M, (int)N, (int)K, (const cplx*)A_dev, (const cplx*)B_dev, (cplx*)C_dev,
+             three != 0);
     NC_ABI_END
     return g_status;
 }

@@ -107,6 +107,7 @@ struct Context {
     double profile_min_flops = 1e9;
     std::vector<cudaEvent_t> prof_start, prof_stop;
     std::vector<double> prof_flops;
+    std::vector<int> prof_kind;   // 0: FP64 DMMA complex GEMM, 1: tcgen05 3xTF32 GEMM
     size_t prof_used = 0;
     Context();
     ~Context();

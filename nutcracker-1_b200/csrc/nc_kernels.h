@@ -7,6 +7,32 @@
 
 namespace nc {
 
+// Runs launch(); when ctx.profile is on and the work is at least
+// profile_min_flops, brackets it with CUDA events on ctx.stream and records
+// (flops, kind) for nc_profile_end / nc_profile_query.
+template <typename F>
+void profile_launch(Context& ctx, double flops, int kind, F&& launch) {
+    if (!ctx.profile || flops < ctx.profile_min_flops) {
+        launch();
+        return;
+    }
+    if (ctx.prof_used == ctx.prof_start.size()) {
+        cudaEvent_t a, b;
+        NC_CUDA(cudaEventCreate(&a));
+        NC_CUDA(cudaEventCreate(&b));
+        ctx.prof_start.push_back(a);
+        ctx.prof_stop.push_back(b);
+        ctx.prof_flops.push_back(0);
+        ctx.prof_kind.push_back(0);
+    }
+    const size_t i = ctx.prof_used++;
+    ctx.prof_flops[i] = flops;
+    ctx.prof_kind[i] = kind;
+    NC_CUDA(cudaEventRecord(ctx.prof_start[i], ctx.stream));
+    launch();
+    NC_CUDA(cudaEventRecord(ctx.prof_stop[i], ctx.stream));
+}
+
 enum Op { OP_N = 0, OP_T = 1, OP_C = 2 };
 
 struct ZGemmParams {
@@ -120,6 +146,53 @@ int convert_vectors_to_reflectors_dev(Context& ctx, long long m, int n, cplx* A,
 // triangle of A; optional explicit Q (m x n) and R (n x n, zeros below,
 // conjugated if conjR).
 void householder_qr(Context& ctx, int m, int n, cplx* A, cplx* Q, cplx* R, bool conjR);
+
+// ---- tcgen05 3xTF32 complex GEMM (tc32.cu) ---------------------------------
+// One operand of the real GEMM: rows x Kr floats, Kr contiguous, row stride
+// ld floats, batch planes sbatch floats apart (0: shared by every batch),
+// held as the TF32 pair big + small.
+struct TcOperand {
+    const float* big = nullptr;
+    const float* small = nullptr;
+    long long ld = 0, sbatch = 0;
+};
+// D[z] = sum_segments A_s[z] B_s[z]^T (M x Nr, FP32 accumulate), read as
+// complex (columns 2n, 2n+1 = Re, Im of column n) and stored to
+// C[z*sz + m*sm + n*sn] as complex128 (c_fp64) or complex64.
+struct TcGemm {
+    TcOperand A, B;
+    int M = 0, Nr = 0, Kr = 0, batch = 1;
+    void* C = nullptr;
+    long long sm = 0, sn = 0, sz = 0;
+    bool c_fp64 = false;
+    bool three = true;   // false: big x big only (one TF32 product)
+};
+void tc_gemm(Context& ctx, const TcGemm& g);
+// Synchronises ctx.stream; raises NC_ERR_TIMEOUT if a tc32 pipeline wait expired.
+void tc_check(Context& ctx);
+
+// ---- precision form of the site products (mixed.cu) ------------------------
+// Tensor-core operands of one site's H_eff (environments expanded once per
+// site) and the scratch of one product, all inside one float buffer of
+// mixed_heff_floats() elements.
+struct MixedHeff {
+    int bl = 0, br = 0;
+    MpoSite op;
+    long long ldL = 0, ldR = 0, ldX = 0, ldU = 0;
+    float *Lb = nullptr, *Ls = nullptr;   // stage-A B operand: rows 2*bl*cl, K 2*bl
+    float *Rb = nullptr, *Rs = nullptr;   // stage-C B operand: rows 2*br, K 2*br*cr
+    float *Xb = nullptr, *Xs = nullptr;   // stage-A A operand: d planes of br rows
+    float2* T = nullptr;                  // stage-A output (br, bl*cl, d) complex64
+    float *Ub = nullptr, *Us = nullptr;   // stage-C A operand: d planes of bl rows
+};
+size_t mixed_heff_floats(int bl, int br, const MpoSite& op);
+void mixed_heff_prepare(Context& ctx, int bl, int br, const MpoSite& op, const cplx* L, const cplx* R,
+                        float* buf, MixedHeff* h);
+// y = H_eff x (x, y complex128 (br,bl,d)) with 3xTF32 tensor-core contractions.
+void heff_apply_mixed(Context& ctx, const MixedHeff& h, const cplx* x, cplx* y);
+// C (M x N) = A (M x K) B (K x N), column-major complex128, through tc_gemm;
+// three = false uses one TF32 product.  Synchronises and checks tc_check.
+void tc_zgemm(Context& ctx, int M, int N, int K, const cplx* A, const cplx* B, cplx* C, bool three);
 // A (bm,bl,dl) -> normA left-normalised; B (br,bm,dr) absorbs the factor.
 void gauge_right(Context& ctx, int bl, int bm, int br, int dl, int dr, const cplx* A, const cplx* B,
                  cplx* normA, cplx* denormB);

@@ -245,23 +245,7 @@ void zgemm_ctx(const ZGemmParams& p_in, Context& ctx);
 
 void zgemm(const ZGemmParams& p, Context& ctx) {
     const double flops = 8.0 * p.M * (double)p.N * p.K * p.batch;
-    if (!ctx.profile || flops < ctx.profile_min_flops) {
-        zgemm_ctx(p, ctx);
-        return;
-    }
-    if (ctx.prof_used == ctx.prof_start.size()) {
-        cudaEvent_t a, b;
-        NC_CUDA(cudaEventCreate(&a));
-        NC_CUDA(cudaEventCreate(&b));
-        ctx.prof_start.push_back(a);
-        ctx.prof_stop.push_back(b);
-        ctx.prof_flops.push_back(0);
-    }
-    const size_t i = ctx.prof_used++;
-    ctx.prof_flops[i] = flops;
-    NC_CUDA(cudaEventRecord(ctx.prof_start[i], ctx.stream));
-    zgemm_ctx(p, ctx);
-    NC_CUDA(cudaEventRecord(ctx.prof_stop[i], ctx.stream));
+    profile_launch(ctx, flops, 0, [&] { zgemm_ctx(p, ctx); });
 }
 
 namespace {

@@ -1,0 +1,77 @@
+"""tcgen05 3xTF32 tensor-core path against FP64.
+
+`nc_tc_zgemm_dev` is the complex GEMM under the precision form (each operand
+split into two TF32 halves, three products, FP32 accumulation in tensor
+memory); `nc_heff_apply_mixed_dev` is the precision-form H_eff product.  Both
+are compared with FP64 results on the same device inputs: the GEMM with
+torch's complex128 matmul, the H_eff product with the FP64 entry point
+`nc_heff_apply_dev` (itself pinned to the oracle in test_gpu_contract.py).
+Sizes cover full tiles, ragged M/N/K edges, a single row and a long K.
+"""
+import ctypes as ct
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL_3X = 2e-6     # relative Frobenius error of 3xTF32 (chunked FP32 accumulation); measured ~7e-7
+TOL_1X = 1e-2     # one TF32 product (10-bit mantissa): loose upper bound
+
+
+def _p(t):
+    return ct.c_void_p(t.data_ptr())
+
+
+def _rel(got, want):
+    import torch
+    return (torch.linalg.norm(got - want) / torch.linalg.norm(want)).item()
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 128, 16), (256, 128, 64), (200, 70, 33), (1, 5, 3),
+                                   (300, 260, 1000), (64, 1, 257)])
+def test_tc_zgemm_matches_fp64(M, N, K):
+    import torch
+
+    import nutcracker_b200 as nb
+
+    g = torch.Generator(device="cuda").manual_seed(7 * M + 3 * N + K)
+    A_cm = torch.randn(K, M, dtype=torch.complex128, device="cuda", generator=g)   # column-major M x K
+    B_cm = torch.randn(N, K, dtype=torch.complex128, device="cuda", generator=g)   # column-major K x N
+    ref = A_cm.T @ B_cm.T
+    errs = []
+    for three in (1, 0):
+        C_cm = torch.full((N, M), float("nan"), dtype=torch.complex128, device="cuda")
+        st = nb.lib.nc_tc_zgemm_dev(M, N, K, _p(A_cm), _p(B_cm), _p(C_cm), three)
+        assert st == 0, nb.lib.nc_last_error()
+        errs.append(_rel(C_cm.T, ref))
+    err3, err1 = errs
+    assert err3 <= TOL_3X, err3
+    assert err1 <= TOL_1X, err1
+    assert err3 * 10 < err1, (err3, err1)   # the small halves carry real precision
+
+
+@pytest.mark.parametrize("bl,br", [(96, 96), (40, 72), (130, 33)])
+def test_mixed_heff_matches_fp64(bl, br):
+    import torch
+
+    import nutcracker_b200 as nb
+    from nutcracker_b200 import operators
+
+    assert nb.lib.nc_set_stream(ct.c_void_p(torch.cuda.current_stream().cuda_stream)) == 0
+    op = operators.heisenberg(4)[1]
+    W = torch.from_numpy(op.W.ravel(order="F")).cuda()
+    idx = torch.from_numpy(op.idx.ravel(order="F").astype(np.int32)).cuda()
+    g = torch.Generator(device="cuda").manual_seed(bl * 1000 + br)
+    L = torch.randn(bl * bl * op.cl, dtype=torch.complex128, device="cuda", generator=g)
+    R = torch.randn(br * br * op.cr, dtype=torch.complex128, device="cuda", generator=g)
+    x = torch.randn(br * bl * op.d, dtype=torch.complex128, device="cuda", generator=g)
+    y64 = torch.empty_like(x)
+    ymx = torch.full_like(x, float("nan"))
+    args = (bl, br, op.cl, op.cr, op.d, op.nnz, _p(idx), _p(W), _p(L), _p(R), _p(x))
+    assert nb.lib.nc_heff_apply_dev(*args, _p(y64)) == 0, nb.lib.nc_last_error()
+    assert nb.lib.nc_heff_apply_mixed_dev(*args, _p(ymx)) == 0, nb.lib.nc_last_error()
+    torch.cuda.synchronize()
+    assert nb.lib.nc_use_own_stream() == 0
+    err = _rel(ymx, y64)
+    assert err <= TOL_3X, err
