@@ -75,6 +75,16 @@ int nc_heff_apply_mixed_dev(uint32_t bl, uint32_t br, uint32_t cl, uint32_t cr, 
                             const uint32_t* idx_dev, const void* W_dev, const void* L_dev,
                             const void* R_dev, const void* x_dev, void* y_dev);
 
+/* Device-pointer environment update for one site: side 0 is
+   contract_sos_left (L (bl,bl,cl) -> L' (br,br,cr), core.f95:623-677),
+   side 1 is contract_sos_right (R (br,br,cr) -> R' (bl,bl,cl),
+   core.f95:679-848); psi (br,bl,d).  mixed = 0 runs the FP64 path, mixed = 1
+   the precision form (3xTF32 tensor-core contractions, FP64 input/output;
+   synchronises this thread's stream).  Returns a status code. */
+int nc_env_update_dev(int side, int mixed, uint32_t bl, uint32_t br, uint32_t cl, uint32_t cr, uint32_t d,
+                      uint32_t nnz, const uint32_t* idx_dev, const void* W_dev, const void* env_dev,
+                      const void* psi_dev, void* out_dev);
+
 /* C = A B for column-major complex128 device matrices A (M x K), B (K x N),
    C (M x N) on the tcgen05 tensor cores: 3xTF32 when `three` is nonzero,
    else one TF32 product.  The GEMM under the precision form, exposed for
@@ -304,6 +314,10 @@ typedef struct {
     uint64_t seed;                    /* random initial states */
     uint32_t strict;                  /* nonzero: a failed site solve is an error */
     uint32_t time_phases;             /* nonzero: synchronise and time each phase (diagnostics) */
+    uint32_t precision;               /* 0: plain FP64 form (default); 1: precision form: sweeps with
+                                         3xTF32 tensor-core contractions (FP64 Krylov, eigenproblem
+                                         and energies), and sweep_until_converged closes with FP64
+                                         refinement sweeps to the options' thresholds */
 } nc_chain_options;
 
 /* One MPO site (OperatorSite, tensors.hpp:1641-1854): indices (2,nnz)
@@ -323,6 +337,8 @@ typedef struct {
     /* seconds spent per phase when time_phases is set: site solves, gauge
        moves, environment updates, projector matrices */
     double seconds_solve, seconds_gauge, seconds_environment, seconds_projector;
+    uint64_t mixed_sweeps;            /* sweeps run in the precision form */
+    uint32_t precision;               /* current precision (0 FP64, 1 mixed) */
 } nc_chain_info;
 
 typedef struct nc_chain nc_chain;
@@ -344,6 +360,11 @@ int nc_chain_optimize_site(nc_chain* chain);                 /* base_chain.cpp:8
 int nc_chain_perform_optimization_sweep(nc_chain* chain);    /* chain.cpp:147-163 */
 int nc_chain_sweep_until_converged(nc_chain* chain);         /* base_chain.cpp:112-123 */
 int nc_chain_optimize_chain(nc_chain* chain);                /* base_chain.cpp:64-79 */
+/* No counterpart in the reference: switch the precision of the following
+   sweeps (0 FP64, 1 precision form).  Going back to FP64 rebuilds every
+   environment in FP64 and resets the energy to the FP64 expectation value
+   of the current state. */
+int nc_chain_set_precision(nc_chain* chain, uint32_t precision);
 int nc_chain_increase_bandwidth_dimension(nc_chain* chain, uint32_t new_dimension); /* chain.cpp:75-122 */
 int nc_chain_construct_and_add_projector_from_state(nc_chain* chain);  /* chain.cpp:63-73 */
 /* solveForEigenvalues (chain.cpp:292-310): `eigenvalues` receives n levels. */

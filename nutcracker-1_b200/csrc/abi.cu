@@ -216,6 +216,30 @@ int nc_heff_apply_mixed_dev(uint32_t bl, uint32_t br, uint32_t cl, uint32_t cr, 
     return g_status;
 }
 
+int nc_env_update_dev(int side, int mixed, uint32_t bl, uint32_t br, uint32_t cl, uint32_t cr, uint32_t d,
+                      uint32_t nnz, const uint32_t* idx_dev, const void* W_dev, const void* env_dev,
+                      const void* psi_dev, void* out_dev) {
+    NC_ABI_BEGIN
+    NC_ARG(side == 0 || side == 1, "side must be 0 (left) or 1 (right)");
+    Context& ctx = Context::get();
+    MpoSite op;
+    op.d = (int)d; op.cl = (int)cl; op.cr = (int)cr; op.nnz = (int)nnz;
+    op.idx = idx_dev; op.W = (const cplx*)W_dev;
+    const cplx* env = (const cplx*)env_dev;
+    const cplx* psi = (const cplx*)psi_dev;
+    cplx* out = (cplx*)out_dev;
+    if (side == 0) {
+        if (mixed) sos_left_mixed(ctx, bl, br, op, env, psi, out);
+        else sos_left(ctx, bl, br, op, env, psi, out);
+    } else {
+        if (mixed) sos_right_mixed(ctx, bl, br, op, env, psi, out);
+        else sos_right(ctx, bl, br, op, env, psi, out);
+    }
+    if (mixed) tc_check(ctx);
+    NC_ABI_END
+    return g_status;
+}
+
 int nc_tc_zgemm_dev(uint32_t M, uint32_t N, uint32_t K, const void* A_dev, const void* B_dev, void* C_dev,
                     int three) {
     NC_ABI_BEGIN

@@ -115,6 +115,10 @@ struct Chain {
     bool optimized = false;
     uint64_t seed_counter = 0;
     ChainStats stats;
+    // precision form: 0 = FP64 sweeps, 1 = 3xTF32 tensor-core products
+    int prec = 0;
+    DevBuf mixbuf;       // MixedHeff operands of the current site (float storage)
+    MixedHeff mh;
 
     Chain(Context& c, int n, const OperatorSiteDesc* sites, const ChainOptions& o) : ctx(c), opt(o), N(n) {
         NC_ARG(N >= 1, "chain needs at least one site");
@@ -137,6 +141,8 @@ struct Chain {
             phys.push_back((int)s.d);
         }
         NC_ARG(ops.front()->dev.cl == 1 && ops.back()->dev.cr == 1, "operator boundary dimensions must be 1");
+        NC_ARG(opt.precision == 0 || opt.precision == 1, "precision must be 0 (FP64) or 1 (mixed)");
+        prec = opt.precision;
         max_bandwidth = maximum_bandwidth_dimension(phys);
         ctx.krylov_dim = opt.krylov_dim;
         reset();
@@ -227,14 +233,16 @@ struct Chain {
 
     // Right environments (and overlap environments) of site i-1 from site i.
     void absorb_right(int i) {
-        sos_right(ctx, bl(i), br(i), op(i), Renv[i].p, site[i].p, Renv[i - 1].p);
+        if (prec) sos_right_mixed(ctx, bl(i), br(i), op(i), Renv[i].p, site[i].p, Renv[i - 1].p);
+        else sos_right(ctx, bl(i), br(i), op(i), Renv[i].p, site[i].p, Renv[i - 1].p);
         for (size_t p = 0; p < projectors.size(); ++p) {
             const ProjSite& ps = projectors[p][i];
             vs_right(ctx, ps.bl, ps.br, bl(i), br(i), phys[i], Rov[p][i].p, ps.right.p, site[i].p, Rov[p][i - 1].p);
         }
     }
     void absorb_left(int i) {
-        sos_left(ctx, bl(i), br(i), op(i), Lenv[i].p, site[i].p, Lenv[i + 1].p);
+        if (prec) sos_left_mixed(ctx, bl(i), br(i), op(i), Lenv[i].p, site[i].p, Lenv[i + 1].p);
+        else sos_left(ctx, bl(i), br(i), op(i), Lenv[i].p, site[i].p, Lenv[i + 1].p);
         for (size_t p = 0; p < projectors.size(); ++p) {
             const ProjSite& ps = projectors[p][i];
             vs_left(ctx, ps.bl, ps.br, bl(i), br(i), phys[i], Lov[p][i].p, ps.left.p, site[i].p, Lov[p][i + 1].p);
@@ -330,7 +338,9 @@ struct Chain {
             move_to(0);
         }
         double e = expectation_value();
-        if (std::fabs(last_expectation.y) / std::fabs(std::hypot(last_expectation.x, last_expectation.y)) > 1e-10)
+        // environments built in the precision form carry ~1e-7 relative error
+        const double imag_tol = prec ? kMixedSanity : 1e-10;
+        if (std::fabs(last_expectation.y) / std::fabs(std::hypot(last_expectation.x, last_expectation.y)) > imag_tol)
             throw Error(NC_ERR_NUMERIC, "initial chain energy is not real");
         energy = e;
     }
@@ -397,12 +407,22 @@ struct Chain {
         EigenStats es;
         DevProjector P = pm;
         if (P.nproj == 0) { P.n = n; P.orth_dim = n; }
-        int info = nc::optimize_site(ctx, bl(cur), br(cur), op(cur), Lenv[cur].p, Renv[cur].p, P, opt.mode,
-                                 opt.site_convergence_threshold, (int)opt.maximum_number_of_iterations,
-                                 site[cur].p, spare_a.p, &ev, &normal, &es);
+        const MixedHeff* mixed = nullptr;
+        if (prec) {
+            const size_t floats = mixed_heff_floats(bl(cur), br(cur), op(cur));
+            mixbuf.ensure((floats + 3) / 4);
+            mixed_heff_prepare(ctx, bl(cur), br(cur), op(cur), Lenv[cur].p, Renv[cur].p,
+                               reinterpret_cast<float*>(mixbuf.p), &mh);
+            mixed = &mh;
+        }
+        const double site_tol = prec ? std::max(opt.site_convergence_threshold, kMixedSiteTol)
+                                     : opt.site_convergence_threshold;
+        int info = nc::optimize_site(ctx, bl(cur), br(cur), op(cur), Lenv[cur].p, Renv[cur].p, P, opt.mode, site_tol,
+                                     (int)opt.maximum_number_of_iterations, site[cur].p, spare_a.p, &ev, &normal, &es,
+                                     mixed);
         stats.matvecs += es.matvecs;
         stats.site_solves++;
-        const double sanity = opt.sanity_check_threshold;
+        const double sanity = prec ? std::max(opt.sanity_check_threshold, kMixedSanity) : opt.sanity_check_threshold;
         int failure = 0;
         if (info == -14) failure = NC_FAIL_UNABLE_TO_CONVERGE;
         else if (info == 10) failure = NC_FAIL_TOO_MANY_PROJECTORS;
@@ -412,7 +432,8 @@ struct Chain {
             // sanity checks of optimizer.cpp:266-309 on the new site
             ArenaFrame f(ctx.arena);
             cplx* r = ctx.arena.alloc_n<cplx>(1);
-            expectation_dev(ctx, bl(cur), br(cur), op(cur), Lenv[cur].p, spare_a.p, Renv[cur].p, r);
+            if (prec) expectation_mixed(ctx, mh, spare_a.p, r);
+            else expectation_dev(ctx, bl(cur), br(cur), op(cur), Lenv[cur].p, spare_a.p, Renv[cur].p, r);
             cplx ex = read_scalar(ctx, r);
             double overlap = (pm.nproj > 0) ? overlap_with_projectors(ctx, pm, spare_a.p) : 0.0;
             // outsideTolerance on complex numbers (utilities.hpp:418-420 with |.| = modulus)
@@ -433,7 +454,7 @@ struct Chain {
         }
         // acceptance rule (base_chain.cpp:97-103)
         if ((energy >= 0 && ev >= 0) || (energy <= 0 && ev <= 0) ||
-            outside_tolerance(std::fabs(energy), std::fabs(ev), opt.sanity_check_threshold)) {
+            outside_tolerance(std::fabs(energy), std::fabs(ev), sanity)) {
             energy = ev;
             std::swap(site[cur], spare_a);
         }
@@ -454,10 +475,51 @@ struct Chain {
         while (cur + 1 < N) { move(+1); optimize_site(); }
         while (cur > 0) { move(-1); optimize_site(); }
         while (cur < start) { move(+1); optimize_site(); }
+        if (prec) {
+            tc_check(ctx);
+            stats.mixed_sweeps++;
+        }
         stats.sweeps++;
     }
 
     void sweep_until_converged() {
+        if (prec) {
+            // precision form: mixed sweeps to kMixedSweepTol, then FP64
+            // sweeps (the refinement) to the options' threshold
+            double prev = energy;
+            perform_optimization_sweep();
+            double now = energy;
+            for (int count = 1; count < kMixedMaxSweeps && outside_tolerance(prev, now, kMixedSweepTol); ++count) {
+                perform_optimization_sweep();
+                prev = now;
+                now = energy;
+            }
+            prec = 0;
+            try {
+                refresh_environments();
+                sweep_until_converged_fp64();
+            } catch (...) {
+                prec = 1;
+                throw;
+            }
+            prec = 1;
+            return;
+        }
+        sweep_until_converged_fp64();
+    }
+
+    // Rebuild every environment for the current state at the current
+    // precision and take the current site's expectation value as the energy
+    // reference (used when the mixed sweeps hand over to the FP64 ones, whose
+    // regression checks must not compare against mixed-precision energies).
+    void refresh_environments() {
+        for (int i = 0; i < cur; ++i) absorb_left(i);
+        for (int i = N - 1; i > cur; --i) absorb_right(i);
+        energy = expectation_value();
+        optimized = false;
+    }
+
+    void sweep_until_converged_fp64() {
         // base_chain.cpp:112-123
         double prev = energy;
         perform_optimization_sweep();
@@ -609,6 +671,7 @@ ChainOptions to_options(const nc_chain_options* o) {
     c.seed = o->seed;
     c.strict = o->strict != 0;
     c.time_phases = o->time_phases != 0;
+    c.precision = (int)o->precision;
     return c;
 }
 }  // namespace
@@ -700,6 +763,14 @@ int nc_chain_solve_for_eigenvalues(nc_chain* c, uint32_t n, double* eigenvalues)
     })
 }
 int nc_chain_get_energy(nc_chain* c, double* energy) { NC_CHAIN_CALL(*energy = ch.energy) }
+int nc_chain_set_precision(nc_chain* c, uint32_t precision) {
+    NC_CHAIN_CALL({
+        NC_ARG(precision <= 1, "precision must be 0 (FP64) or 1 (mixed)");
+        const int was = ch.prec;
+        ch.prec = (int)precision;
+        if (was == 1 && ch.prec == 0) ch.refresh_environments();
+    })
+}
 int nc_chain_compute_expectation_value(nc_chain* c, double* value) { NC_CHAIN_CALL(*value = ch.expectation_value()) }
 
 int nc_chain_get_info(nc_chain* c, nc_chain_info* info) {
@@ -720,6 +791,8 @@ int nc_chain_get_info(nc_chain* c, nc_chain_info* info) {
         info->seconds_gauge = ch.stats.t_gauge;
         info->seconds_environment = ch.stats.t_env;
         info->seconds_projector = ch.stats.t_proj;
+        info->mixed_sweeps = ch.stats.mixed_sweeps;
+        info->precision = (uint32_t)ch.prec;
     })
 }
 

@@ -377,7 +377,7 @@ struct Filter {
 
 int optimize_site(Context& ctx, int bl, int br, const MpoSite& op, const cplx* L, const cplx* R,
                   const DevProjector& P, int which, double tol, int maxit, const cplx* guess,
-                  cplx* result, double* eigenvalue, double* normal, EigenStats* stats) {
+                  cplx* result, double* eigenvalue, double* normal, EigenStats* stats, const MixedHeff* mixed) {
     const long long n = (long long)br * bl * op.d;
     const long long orth_dim = P.nproj ? P.orth_dim : n;
     EigenStats st;
@@ -390,7 +390,12 @@ int optimize_site(Context& ctx, int bl, int br, const MpoSite& op, const cplx* L
     if (orth_dim < n && overlap > 1e-7) return 11;
 
     ArenaFrame frame(ctx.arena);
-    cplx* ws = ctx.arena.alloc_n<cplx>(heff_workspace_elems(bl, br, op));
+    cplx* ws = mixed ? nullptr : ctx.arena.alloc_n<cplx>(heff_workspace_elems(bl, br, op));
+    // y = H_eff x: FP64, or the precision form when `mixed` is given
+    auto apply = [&](const cplx* x, cplx* y) {
+        if (mixed) heff_apply_mixed(ctx, *mixed, x, y);
+        else heff_apply(ctx, bl, br, op, L, R, x, y, ws);
+    };
     Filter filt;
     if (P.nproj > 0 && orth_dim < n) {
         filt.r = (int)(n - orth_dim);
@@ -408,7 +413,7 @@ int optimize_site(Context& ctx, int bl, int br, const MpoSite& op, const cplx* L
         cplx* M = ctx.arena.alloc_n<cplx>((size_t)k * k);
         for (int q = 0; q < k; ++q) {
             unproject_unit(ctx, P, q, B + (size_t)q * n);
-            heff_apply(ctx, bl, br, op, L, R, B + (size_t)q * n, HB_ + (size_t)q * n, ws);
+            apply(B + (size_t)q * n, HB_ + (size_t)q * n);
         }
         for (int q = 0; q < k; ++q) multi_dotc(ctx, n, k, B, HB_ + (size_t)q * n, M + (size_t)q * k);
         double* ev = ctx.arena.alloc_n<double>(1);
@@ -473,7 +478,7 @@ int optimize_site(Context& ctx, int bl, int br, const MpoSite& op, const cplx* L
     int j = 0;
     for (;;) {
         cplx* vj = V + (size_t)j * n;
-        heff_apply(ctx, bl, br, op, L, R, vj, w, ws);
+        apply(vj, w);
         filt.apply(ctx, n, w);
         ++st.matvecs;
         orthogonalise(w, j + 1);

@@ -36,7 +36,18 @@ struct ChainOptions {
     uint64_t seed = 1;
     bool strict = false;                // raise on a site failure instead of keeping the old site
     bool time_phases = false;           // synchronise and time each phase
+    int precision = 0;                  // 0: all FP64; 1: precision form (mixed sweeps + FP64 refinement)
 };
+
+// Thresholds of the mixed sweeps (the FP64 refinement uses the options'):
+// the 3xTF32 products carry ~1e-6 relative error, so the Lanczos residual is
+// taken to 1e-5 (the Ritz value is still accurate to ~1e-10 relative), the
+// eigenvalue/expectation sanity check to 1e-5, and the mixed sweeps stop at a
+// 1e-7 relative energy change or after kMixedMaxSweeps sweeps.
+constexpr double kMixedSiteTol = 1e-5;
+constexpr double kMixedSanity = 1e-5;
+constexpr double kMixedSweepTol = 1e-7;
+constexpr int kMixedMaxSweeps = 50;
 
 struct OperatorSiteDesc {
     uint32_t d, cl, cr, nnz;
@@ -45,7 +56,7 @@ struct OperatorSiteDesc {
 };
 
 struct ChainStats {
-    uint64_t sweeps = 0, site_solves = 0, matvecs = 0, moves = 0, failures = 0;
+    uint64_t sweeps = 0, site_solves = 0, matvecs = 0, moves = 0, failures = 0, mixed_sweeps = 0;
     int last_failure = 0;
     double t_solve = 0, t_gauge = 0, t_env = 0, t_proj = 0;
 };

@@ -190,6 +190,11 @@ void mixed_heff_prepare(Context& ctx, int bl, int br, const MpoSite& op, const c
                         float* buf, MixedHeff* h);
 // y = H_eff x (x, y complex128 (br,bl,d)) with 3xTF32 tensor-core contractions.
 void heff_apply_mixed(Context& ctx, const MixedHeff& h, const cplx* x, cplx* y);
+// <psi|H_eff|psi> with the precision-form product.
+void expectation_mixed(Context& ctx, const MixedHeff& h, const cplx* psi, cplx* result);
+// Environment updates (sos_left / sos_right) in the precision form.
+void sos_left_mixed(Context& ctx, int bl, int br, const MpoSite& op, const cplx* L, const cplx* psi, cplx* Lnew);
+void sos_right_mixed(Context& ctx, int bl, int br, const MpoSite& op, const cplx* R, const cplx* psi, cplx* Rnew);
 // C (M x N) = A (M x K) B (K x N), column-major complex128, through tc_gemm;
 // three = false uses one TF32 product.  Synchronises and checks tc_check.
 void tc_zgemm(Context& ctx, int M, int N, int K, const cplx* A, const cplx* B, cplx* C, bool three);
@@ -218,9 +223,13 @@ struct EigenStats {
 };
 
 // The site eigen-solve of core.f95:1911-2609 on the device.  Returns the
-// reference's info code (0, 5, 10, 11, -14).
+// reference's info code (0, 5, 10, 11, -14).  With `mixed` (prepared for the
+// same L, R) every H_eff product runs in the precision form; the Krylov
+// basis, its reorthogonalisation and the projected eigenproblem stay FP64.
 int optimize_site(Context& ctx, int bl, int br, const MpoSite& op, const cplx* L, const cplx* R,
                   const DevProjector& P, int which, double tol, int maxit, const cplx* guess,
-                  cplx* result, double* eigenvalue, double* normal, EigenStats* stats);
+                  cplx* result, double* eigenvalue, double* normal, EigenStats* stats,
+                  const MixedHeff* mixed = nullptr);
+
 
 }  // namespace nc

@@ -28,6 +28,7 @@ class nc_chain_options(ct.Structure):
         ("seed", ct.c_uint64),
         ("strict", ct.c_uint32),
         ("time_phases", ct.c_uint32),
+        ("precision", ct.c_uint32),
     ]
 
 
@@ -60,6 +61,8 @@ class nc_chain_info(ct.Structure):
         ("seconds_gauge", ct.c_double),
         ("seconds_environment", ct.c_double),
         ("seconds_projector", ct.c_double),
+        ("mixed_sweeps", ct.c_uint64),
+        ("precision", ct.c_uint32),
     ]
 
 
@@ -73,6 +76,7 @@ for _f in ("nc_chain_reset", "nc_chain_optimize_site", "nc_chain_perform_optimiz
     getattr(lib, _f).restype = ct.c_int
 lib.nc_chain_increase_bandwidth_dimension.argtypes = [ct.c_void_p, ct.c_uint32]
 lib.nc_chain_move_to.argtypes = [ct.c_void_p, ct.c_uint32]
+lib.nc_chain_set_precision.argtypes = [ct.c_void_p, ct.c_uint32]
 lib.nc_chain_solve_for_eigenvalues.argtypes = [ct.c_void_p, ct.c_uint32, ct.POINTER(ct.c_double)]
 lib.nc_chain_get_energy.argtypes = [ct.c_void_p, ct.POINTER(ct.c_double)]
 lib.nc_chain_compute_expectation_value.argtypes = [ct.c_void_p, ct.POINTER(ct.c_double)]
@@ -169,6 +173,10 @@ class Chain:
 
     def construct_and_add_projector_from_state(self):
         self._call(lib.nc_chain_construct_and_add_projector_from_state)
+
+    def set_precision(self, precision):
+        """0: FP64 sweeps; 1: precision form (3xTF32 tensor-core contractions)."""
+        self._call(lib.nc_chain_set_precision, ct.c_uint32(int(precision)))
 
     def move_to(self, i):
         self._call(lib.nc_chain_move_to, ct.c_uint32(int(i)))

@@ -23,6 +23,19 @@ def _p(t):
     return ct.c_void_p(t.data_ptr())
 
 
+@pytest.fixture(autouse=True)
+def _on_torch_stream():
+    """Run the library on torch's current stream, so it sees torch's inputs."""
+    import torch
+
+    import nutcracker_b200 as nb
+
+    assert nb.lib.nc_set_stream(ct.c_void_p(torch.cuda.current_stream().cuda_stream)) == 0
+    yield
+    torch.cuda.synchronize()
+    assert nb.lib.nc_use_own_stream() == 0
+
+
 def _rel(got, want):
     import torch
     return (torch.linalg.norm(got - want) / torch.linalg.norm(want)).item()
@@ -58,7 +71,6 @@ def test_mixed_heff_matches_fp64(bl, br):
     import nutcracker_b200 as nb
     from nutcracker_b200 import operators
 
-    assert nb.lib.nc_set_stream(ct.c_void_p(torch.cuda.current_stream().cuda_stream)) == 0
     op = operators.heisenberg(4)[1]
     W = torch.from_numpy(op.W.ravel(order="F")).cuda()
     idx = torch.from_numpy(op.idx.ravel(order="F").astype(np.int32)).cuda()
@@ -72,6 +84,30 @@ def test_mixed_heff_matches_fp64(bl, br):
     assert nb.lib.nc_heff_apply_dev(*args, _p(y64)) == 0, nb.lib.nc_last_error()
     assert nb.lib.nc_heff_apply_mixed_dev(*args, _p(ymx)) == 0, nb.lib.nc_last_error()
     torch.cuda.synchronize()
-    assert nb.lib.nc_use_own_stream() == 0
     err = _rel(ymx, y64)
+    assert err <= TOL_3X, err
+
+
+@pytest.mark.parametrize("side", [0, 1])
+@pytest.mark.parametrize("bl,br", [(96, 96), (40, 72), (130, 33)])
+def test_mixed_environment_matches_fp64(side, bl, br):
+    import torch
+
+    import nutcracker_b200 as nb
+    from nutcracker_b200 import operators
+
+    op = operators.heisenberg(4)[1]
+    W = torch.from_numpy(op.W.ravel(order="F")).cuda()
+    idx = torch.from_numpy(op.idx.ravel(order="F").astype(np.int32)).cuda()
+    g = torch.Generator(device="cuda").manual_seed(side * 7 + bl * 1000 + br)
+    n_in, n_out = (bl * bl * op.cl, br * br * op.cr) if side == 0 else (br * br * op.cr, bl * bl * op.cl)
+    env = torch.randn(n_in, dtype=torch.complex128, device="cuda", generator=g)
+    psi = torch.randn(br * bl * op.d, dtype=torch.complex128, device="cuda", generator=g)
+    o64 = torch.empty(n_out, dtype=torch.complex128, device="cuda")
+    omx = torch.full_like(o64, float("nan"))
+    args = (bl, br, op.cl, op.cr, op.d, op.nnz, _p(idx), _p(W), _p(env), _p(psi))
+    assert nb.lib.nc_env_update_dev(side, 0, *args, _p(o64)) == 0, nb.lib.nc_last_error()
+    assert nb.lib.nc_env_update_dev(side, 1, *args, _p(omx)) == 0, nb.lib.nc_last_error()
+    torch.cuda.synchronize()
+    err = _rel(omx, o64)
     assert err <= TOL_3X, err
