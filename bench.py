@@ -1,18 +1,25 @@
 #!/usr/bin/env python
-"""Benchmark: variational-MPS sweeps per second on the Heisenberg chain.
+"""Benchmark: variational-MPS sweeps per second on the Heisenberg chain,
+precision form (3xTF32 tensor-core contractions) against the plain FP64 form.
 
 Workload (the reference's headline configuration): S=1/2 Heisenberg XXX
 chain H = sum (XX + YY + ZZ), N=100 open sites, d=2, MPO bond dimension 5,
 state bond dimension chi=1024 (reached from a chi=256 warm start, "256 then
-1024"), complex128, seeded random initial MPS, reference tolerances (1e-12).
+1024"), complex128 state, seeded random initial MPS, reference tolerances.
 
 One step = one full optimisation sweep (Chain::performOptimizationSweep,
 chain.cpp:147-163): 198 site eigen-solves, 198 gauge moves and environment
-updates.  ``value`` is sweeps/s with the chain resident in HBM; ``e2e`` is the
-same metric through the public C-ABI with the state uploaded from pinned host
-memory (environments rebuilt) before each sweep and the energy read back
-after it.  Per-site working sets (environments 84 MB each) exceed the 126 MB
-L2 together with the site and scratch tensors, so no L2 flush is inserted.
+updates.  Both forms are timed from the same chi=1024 state (after W FP64
+warm-up sweeps; the precision form gets its own W untimed warm-up sweeps
+before returning to that state).  ``value`` is the precision form's sweeps/s,
+``fp64.value`` the plain form's, ``accuracy`` the energy differences per site
+between the two after the same number of sweeps and after one closing FP64
+sweep on each side (the refinement), so they measure precision alone.
+``e2e`` is the precision form through the public C-ABI with the state
+uploaded from pinned host memory (environments rebuilt) before each sweep
+and the energy read back after it.  Per-site working sets (environments 84 MB
+each) exceed the 126 MB L2 together with the site and scratch tensors, so no
+L2 flush is inserted.
 
 ``--impl reference`` times the CPU restatement of the reference path
 (numpy/scipy on all host cores: reference-ordered zgemm H_eff products,
@@ -39,7 +46,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "nutcracker-1_b200"))
 
-METRIC = "sweeps/s @N=100 chi=1024 Heisenberg (complex128, plain FP64 form)"
+METRIC = "sweeps/s @N=100 \u03c7=1024 mixed vs FP64 GPU at |\u0394E|/N\u22641e-9"
 UNIT = "sweeps/s"
 # H_eff products per site step charged to the CPU sample: the mean measured
 # by this GPU path on the same workload in its timed sweeps (1.37; ARPACK
@@ -59,6 +66,9 @@ def parse():
     ap.add_argument("--chi-start", type=int, default=256)
     ap.add_argument("--presweeps", type=int, default=2)
     ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"],
+                    help="both (default): time FP64 and precision-form sweeps from the same state; "
+                         "value is the precision form's")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--phases", action="store_true",
@@ -304,6 +314,37 @@ def run_ours(args, rank, world):
         if dist:
             td.barrier()
 
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        td.all_reduce(t, op=td.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed_sweeps(chain, steps):
+        barrier()
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.nvtx.range_push("timed")
+        ev0.record(stream)
+        for _ in range(steps):
+            chain.perform_optimization_sweep()
+        ev1.record(stream)
+        torch.cuda.nvtx.range_pop()
+        torch.cuda.synchronize()
+        barrier()
+        return max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+
+    def query(kind):
+        n, ms, fl = ct.c_uint64(), ct.c_double(), ct.c_double()
+        nb.lib.nc_profile_query(kind, ct.byref(n), ct.byref(ms), ct.byref(fl))
+        return int(n.value), ms.value / 1e3, fl.value
+
+    def end_profile():
+        n, ms, fl = ct.c_uint64(), ct.c_double(), ct.c_double()
+        nb.lib.nc_profile_end(ct.byref(n), ct.byref(ms), ct.byref(fl))
+
     ops = operators.heisenberg(args.sites)
     chain = Chain(ops, initial_bandwidth_dimension=args.chi_start, seed=args.seed + 7919 * rank,
                   time_phases=1 if args.phases else 0)
@@ -312,46 +353,61 @@ def run_ours(args, rank, world):
     chain.increase_bandwidth_dimension(args.chi)
     for _ in range(args.warmup):
         chain.perform_optimization_sweep()
-    info0 = chain.info()
-
+    # common start of both forms: the same chi=1024 state, so the energy
+    # differences below are due to precision alone
+    start = chain.state_sites()
+    n = args.sites
+    want64 = args.precision in ("both", "fp64")
+    wantmx = args.precision in ("both", "mixed")
     clocks = ClockSampler(local)
     clocks.start()
-    barrier()
-    torch.cuda.synchronize()
-    launches0 = nb.launch_count()
-    nb.lib.nc_profile_begin(ct.c_double(1e9))
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    torch.cuda.nvtx.range_push("timed")
-    ev0.record(stream)
-    for _ in range(args.steps):
+    res = {}
+
+    if want64:
+        chain.set_precision(0)
+        chain.set_state(start)
+        info0 = chain.info()
+        launches0 = nb.launch_count()
+        nb.lib.nc_profile_begin(ct.c_double(1e9))
+        t64 = timed_sweeps(chain, args.steps)
+        g64 = query(0)
+        end_profile()
+        info1 = chain.info()
+        res["fp64"] = {"seconds": t64, "launches": nb.launch_count() - launches0, "gemm": g64,
+                       "energy": chain.get_energy(), "info0": info0, "info1": info1}
+        chain.perform_optimization_sweep()            # one more FP64 sweep: the reference for the closing sweep
+        res["fp64"]["energy_plus1"] = chain.get_energy()
+
+    if wantmx:
+        chain.set_precision(1)
+        for _ in range(args.warmup):                  # first-use allocations, tensor maps
+            chain.perform_optimization_sweep()
+        chain.set_state(start)
+        info0 = chain.info()
+        launches0 = nb.launch_count()
+        nb.lib.nc_profile_begin(ct.c_double(1e9))
+        tmx = timed_sweeps(chain, args.steps)
+        gtc = query(1)
+        g64m = query(0)
+        end_profile()
+        info1 = chain.info()
+        res["mixed"] = {"seconds": tmx, "launches": nb.launch_count() - launches0, "tc": gtc, "gemm": g64m,
+                        "energy": chain.get_energy(), "info0": info0, "info1": info1}
+        # closing FP64 sweep (the refinement): FP64 environments, then one sweep
+        chain.set_precision(0)
+        res["mixed"]["energy_fp64_expectation"] = chain.get_energy()
         chain.perform_optimization_sweep()
-    ev1.record(stream)
-    torch.cuda.nvtx.range_pop()
-    torch.cuda.synchronize()
-    barrier()
+        res["mixed"]["energy_closed"] = chain.get_energy()
     clk = clocks.stop()
-    elapsed = ev0.elapsed_time(ev1) / 1e3
-    launches = nb.launch_count() - launches0
-    pl, pms, pfl = ct.c_uint64(), ct.c_double(), ct.c_double()
-    nb.lib.nc_profile_end(ct.byref(pl), ct.byref(pms), ct.byref(pfl))
-    info1 = chain.info()
-    energy = chain.get_energy()
 
-    t_max = elapsed
-    if dist:
-        t = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
-        td.all_reduce(t, op=td.ReduceOp.MAX)
-        t_max = float(t.item())
-    value = args.steps * world / t_max
-
-    # e2e: state from pinned host memory -> sweep -> energy back, through the C-ABI
+    # e2e through the public API: state from pinned host memory -> sweep -> energy back
     e2e = None
+    head = "mixed" if wantmx else "fp64"
     if not args.no_e2e:
-        host = chain.state_sites()
-        pinned = [torch.from_numpy(np.ascontiguousarray(s.ravel(order="F"))).pin_memory() for s in host]
+        chain.set_precision(1 if head == "mixed" else 0)
+        pinned = [torch.from_numpy(np.ascontiguousarray(s.ravel(order="F"))).pin_memory() for s in start]
         h2d = sum(p.numel() * 16 for p in pinned)
-        bonds = [int(host[0].shape[1])] + [int(s.shape[0]) for s in host]
+        bonds = [int(start[0].shape[1])] + [int(s.shape[0]) for s in start]
         b = (ct.c_uint32 * len(bonds))(*bonds)
         ptrs = (ct.c_void_p * len(pinned))(*[p.data_ptr() for p in pinned])
         barrier()
@@ -368,16 +424,11 @@ def run_ours(args, rank, world):
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
-        te = e0.elapsed_time(e1) / 1e3
-        if dist:
-            t = torch.tensor([te], device="cuda", dtype=torch.float64)
-            td.all_reduce(t, op=td.ReduceOp.MAX)
-            te = float(t.item())
+        te = max_over_ranks(e0.elapsed_time(e1) / 1e3)
         e2e = {"value": args.steps * world / te, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": 8, "wall_s": time.perf_counter() - t0}
+               "d2h_bytes_per_step": 8, "precision": head, "wall_s": time.perf_counter() - t0}
 
-    # roofline of the dominant kernel: the FP64 DMMA complex GEMM
-    achieved = (pfl.value / (pms.value / 1e3)) / 1e12 if pms.value > 0 else None
+    # FP64 GEMM peak measured live (MEASURED_PEAKS.json has no FP64 entry)
     a = torch.randn(4096, 4096, dtype=torch.complex128, device="cuda")
     bm = torch.randn(4096, 4096, dtype=torch.complex128, device="cuda")
     for _ in range(2):
@@ -390,35 +441,75 @@ def run_ours(args, rank, world):
         a @ bm
     q1.record(stream)
     torch.cuda.synchronize()
-    peak = 8 * 4096 ** 3 * 5 / (q0.elapsed_time(q1) / 1e3) / 1e12
+    peak64 = 8 * 4096 ** 3 * 5 / (q0.elapsed_time(q1) / 1e3) / 1e12
     del a, bm
 
     if rank != 0:
         return
-    matvecs = info1["matvecs"] - info0["matvecs"]
-    solves = info1["site_solves"] - info0["site_solves"]
-    line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "complex128", "data": "synthetic",
-        "config": {"workload": "heisenberg_xxx_N%d_chi%d" % (args.sites, args.chi), "sites": args.sites,
-                   "chi": args.chi, "chi_start": args.chi_start, "d": 2, "mpo_bond": 5,
-                   "precision": "fp64", "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "inputs larger than L2 (84 MB environments per site)"},
-        "e2e": e2e,
-        "gpu_launches": int(launches),
-        "roofline": {"bound": "tensor", "kernel": "zgemm_dmma (FP64 DMMA complex GEMM)",
-                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": (achieved / peak) if achieved else None, "traffic": None,
-                     "peak_source": "cuBLAS zgemm 4096^3 measured in this run (no FP64 entry in MEASURED_PEAKS.json)",
-                     "timed_gemms": int(pl.value), "gemm_seconds": pms.value / 1e3,
-                     "gemm_share_of_step": (pms.value / 1e3) / elapsed if elapsed > 0 else None},
-        "clocks": clk,
-        "chain": {"energy": energy, "energy_per_site": energy / args.sites, "matvecs_per_site": matvecs / max(solves, 1),
-                  "site_solves": solves, "failures": info1["failures"] - info0["failures"],
-                  "phase_seconds": {k: info1["seconds_" + k] - info0["seconds_" + k]
-                                    for k in ("solve", "gauge", "environment", "projector")} if args.phases else None},
-    }
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    peak_tf32 = peaks.get("bf16_tflops", 1590.0) / 2.0
+    peak_src = ("MEASURED_PEAKS.json bf16_tflops (burst) / 2: dense TF32 runs at half the dense BF16 rate"
+                if "bf16_tflops" in peaks else "fallback 1.59 PFLOP/s bf16 / 2")
+
+    def chain_stats(r):
+        i0, i1 = r["info0"], r["info1"]
+        solves = i1["site_solves"] - i0["site_solves"]
+        out = {"energy": r["energy"], "energy_per_site": r["energy"] / n,
+               "matvecs_per_site": (i1["matvecs"] - i0["matvecs"]) / max(solves, 1),
+               "site_solves": solves, "failures": i1["failures"] - i0["failures"]}
+        if args.phases:
+            out["phase_seconds"] = {k: i1["seconds_" + k] - i0["seconds_" + k]
+                                    for k in ("solve", "gauge", "environment", "projector")}
+        return out
+
+    line = {"metric": METRIC, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "data": "synthetic",
+            "config": {"workload": "heisenberg_xxx_N%d_chi%d" % (args.sites, args.chi), "sites": args.sites,
+                       "chi": args.chi, "chi_start": args.chi_start, "d": 2, "mpo_bond": 5,
+                       "precision": head, "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "inputs larger than L2 (84 MB environments per site)"},
+            "e2e": e2e, "clocks": clk}
+    if "fp64" in res:
+        r = res["fp64"]
+        v64 = args.steps * world / r["seconds"]
+        ms, fl = r["gemm"][1], r["gemm"][2]
+        ach = fl / ms / 1e12 if ms > 0 else None
+        line["fp64"] = {"value": v64, "ms_per_step": r["seconds"] / args.steps * 1e3,
+                        "gpu_launches": int(r["launches"]), "chain": chain_stats(r),
+                        "roofline": {"bound": "tensor", "kernel": "zgemm_dmma (FP64 DMMA complex GEMM)",
+                                     "achieved": ach, "peak": peak64, "unit": "TFLOP/s",
+                                     "frac": ach / peak64 if ach else None,
+                                     "peak_source": "cuBLAS zgemm 4096^3 measured in this run",
+                                     "gemm_share_of_step": ms / r["seconds"]}}
+    if "mixed" in res:
+        r = res["mixed"]
+        vmx = args.steps * world / r["seconds"]
+        ms, fl = r["tc"][1], r["tc"][2]
+        ach = fl / ms / 1e12 if ms > 0 else None
+        line.update({"value": vmx, "ms_per_step": r["seconds"] / args.steps * 1e3, "dtype": "3xTF32/f64",
+                     "gpu_launches": int(r["launches"])})
+        line["roofline"] = {"bound": "tensor", "kernel": "tc32_gemm_kernel (tcgen05 kind::tf32, 3xTF32 complex GEMM)",
+                            "achieved": ach, "peak": peak_tf32, "unit": "TFLOP/s",
+                            "frac": ach / peak_tf32 if ach else None, "traffic": None,
+                            "flops_counted": "TF32 tensor work: 2*M*Nr*Kr per segment, 3 segments",
+                            "peak_source": peak_src, "timed_gemms": r["tc"][0],
+                            "gemm_share_of_step": ms / r["seconds"],
+                            "fp64_gemm_share_of_step": r["gemm"][1] / r["seconds"]}
+        line["chain"] = chain_stats(r)
+        acc = {"energy_mixed": r["energy"], "energy_fp64_expectation_of_mixed_state": r["energy_fp64_expectation"],
+               "energy_after_closing_fp64_sweep": r["energy_closed"]}
+        if "fp64" in res:
+            e64, e64p = res["fp64"]["energy"], res["fp64"]["energy_plus1"]
+            acc.update({"energy_fp64_same_sweeps": e64, "energy_fp64_one_more_sweep": e64p,
+                        "dE_per_site_mixed_sweeps": abs(r["energy"] - e64) / n,
+                        "dE_per_site_after_closing_sweep": abs(r["energy_closed"] - e64p) / n,
+                        "speedup_vs_fp64": vmx / line["fp64"]["value"]})
+        line["accuracy"] = acc
+    else:
+        line.update({"value": line["fp64"]["value"], "ms_per_step": line["fp64"]["ms_per_step"],
+                     "dtype": "complex128", "gpu_launches": line["fp64"]["gpu_launches"],
+                     "roofline": line["fp64"]["roofline"], "chain": line["fp64"]["chain"]})
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.sites, args.chi)
     print(json.dumps(line), flush=True)
