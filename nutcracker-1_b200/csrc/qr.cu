@@ -289,11 +289,12 @@ __global__ void __launch_bounds__(4 * NB) build_t_kernel(int nb, const cplx* __r
 // the whole block needs one launch instead of NB/JB panel and update
 // launches.  Column j needs a single cluster-wide reduction: every CTA forms,
 // over its rows below the diagonal,
-//   s_k = sum_r conj(x_r) P(r,k)   for all k   (x = column j)
-// which gives the column norm (k = j), the reflector products with the
-// trailing columns (k > j: w_k = P(j,k) + conj(scale) s_k) and the Gram
-// column of the compact-WY T (k < j: G(k,j) = conj(V(j,k)) + scale conj(s_k)),
-// because v = e_j + scale * x.  Each CTA stores its partial sums (and CTA 0,
+//   s_k = sum_r conj(x_r) P(r,k)   for k >= j   (x = column j)
+// which gives the column norm (k = j) and the reflector products with the
+// trailing columns (k > j: w_k = P(j,k) + conj(scale) s_k), because
+// v = e_j + scale * x; warps whose columns all lie left of j sit the column
+// out (the Gram matrix V^H V of the compact-WY T is one GEMM after the
+// kernel).  Each CTA stores its partial sums (and CTA 0,
 // which holds the pivot rows, row j) into every CTA's shared memory (DSMEM,
 // double-buffered by column parity) and one cluster barrier publishes them;
 // each CTA then reduces the C partials with the same tree, so all CTAs
@@ -308,8 +309,7 @@ constexpr int CQ_MAXR = 128;          // rows per CTA -> mp <= 2048
 constexpr int CQ_RPT = CQ_MAXR / CQ_G;  // rows per thread
 __global__ void __launch_bounds__(CQ_T, 1)
 cluster_block_qr_kernel(int mp, int nb, int rows_per_cta, cplx* __restrict__ A, long long lda,
-                        cplx* __restrict__ V, long long ldv, cplx* __restrict__ tau_out,
-                        cplx* __restrict__ G) {
+                        cplx* __restrict__ V, long long ldv, cplx* __restrict__ tau_out) {
     __shared__ cplx recv[2][CQ_MAXC][NB];   // partial sums by source CTA, per column parity
     __shared__ cplx piv[2][NB];             // pivot row as received, per column parity
     __shared__ cplx pivst[2][NB];           // pivot row staged by its owners (CTA 0)
@@ -341,103 +341,105 @@ cluster_block_qr_kernel(int mp, int nb, int rows_per_cta, cplx* __restrict__ A, 
 
     for (int j = 0; j < nb; ++j) {
         const int p = j & 1;
-        // phase 1: partial sums over this CTA's rows below the diagonal.  Only
-        // CTA 0's first NB rows can lie on or above the diagonal (j < NB).
-        double s0r = 0, s0i = 0, s1r = 0, s1i = 0;
+        // Only columns k >= j take part in column j; a warp whose four
+        // columns all lie left of j (k = 4*warp .. 4*warp + 3) skips it.
+        const bool wactive = 4 * (tid >> 5) + 3 >= j;
+        if (wactive) {
+            // phase 1: partial sums over this CTA's rows below the diagonal.
+            // Only CTA 0's first NB rows can lie on or above the diagonal.
+            double s0r = 0, s0i = 0, s1r = 0, s1i = 0;
 #pragma unroll
-        for (int i = 0; i < CQ_RPT; i += 2) {
-            const int r0 = g + CQ_G * i, r1 = r0 + CQ_G;
-            const cplx x0 = xs[p][r0], x1 = xs[p][r1];
-            const bool u0 = !top || r0 >= NB || r0 > j, u1 = !top || r1 >= NB || r1 > j;
-            if (u0) {
-                s0r = fma(x0.x, a[i].x, fma(x0.y, a[i].y, s0r));
-                s0i = fma(x0.x, a[i].y, fma(-x0.y, a[i].x, s0i));
-            }
-            if (u1) {
-                s1r = fma(x1.x, a[i + 1].x, fma(x1.y, a[i + 1].y, s1r));
-                s1i = fma(x1.x, a[i + 1].y, fma(-x1.y, a[i + 1].x, s1i));
-            }
-        }
-        double sr = s0r + s1r, si = s0i + s1i;
-#pragma unroll
-        for (int o = 1; o < CQ_G; o <<= 1) {
-            sr += __shfl_xor_sync(0xffffffffu, sr, o);
-            si += __shfl_xor_sync(0xffffffffu, si, o);
-        }
-        cplx part = cmake(sr, si);
-        cplx pv = cmake(0, 0);
-        if (k < j) part = cmul(part, colscale[k]);
-        if (top) {
-            pv = pivst[p][k];
-            if (k < j) pv = cmul(pv, colscale[k]);
-        }
-        // phase 2: push to every CTA of the cluster (DSMEM stores), then one
-        // cluster barrier (release/acquire) publishes them
-        for (int d = g; d < C; d += CQ_G) {
-            cluster.map_shared_rank(&recv[p][rank][0], d)[k] = part;
-            if (top) cluster.map_shared_rank(&piv[p][0], d)[k] = pv;
-        }
-        cluster.sync();
-        // phase 3: the CQ_G lanes of column k split the sources; a fixed
-        // reduction tree keeps every CTA bit-identical
-        cplx Sk = cmake(0, 0), Sj = cmake(0, 0);
-        for (int c = g; c < C; c += CQ_G) {
-            Sk = cadd(Sk, recv[p][c][k]);
-            Sj = cadd(Sj, recv[p][c][j]);
-        }
-#pragma unroll
-        for (int o = 1; o < CQ_G; o <<= 1) {
-            Sk.x += __shfl_xor_sync(0xffffffffu, Sk.x, o);
-            Sk.y += __shfl_xor_sync(0xffffffffu, Sk.y, o);
-            Sj.x += __shfl_xor_sync(0xffffffffu, Sj.x, o);
-        }
-        const double xnorm2 = Sj.x;
-        const cplx alpha = piv[p][j];
-        const cplx pk = piv[p][k];
-        cplx t = cmake(0, 0), scale = cmake(1, 0), diag = alpha;
-        const bool reflect = !(xnorm2 == 0.0 && alpha.y == 0.0);
-        if (reflect) {
-            const double beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xnorm2), alpha.x);
-            const cplx den = cmake(alpha.x - beta, alpha.y);
-            const double ib = 1.0 / beta;
-            const double idd = 1.0 / (den.x * den.x + den.y * den.y);
-            t = cmake((beta - alpha.x) * ib, -alpha.y * ib);
-            scale = cmake(den.x * idd, -den.y * idd);
-            diag = cmake(beta, 0);
-        }
-        if (tid == 0) {
-            colscale[j] = scale;
-            taus[j] = t;
-        }
-        if (top && g == 0 && k < j) G[k + (long long)nb * j] = cadd(cconj(pk), cmul(scale, cconj(Sk)));
-        // phase 4: apply H_j^H = I - conj(tau) v v^H to the trailing columns
-        if (reflect && k > j && k < nb) {
-            const cplx cf = cmul(cconj(t), cadd(pk, cmul(cconj(scale), Sk)));
-            const cplx ef = cmul(scale, cf);
-            if (top) {
-#pragma unroll
-                for (int i = 0; i < CQ_RPT; ++i) {
-                    const int r = g + CQ_G * i;
-                    if (r < NB && r == j) a[i] = csub(a[i], cf);
-                    else if (r >= NB || r > j) a[i] = csub(a[i], cmul(xs[p][r], ef));
+            for (int i = 0; i < CQ_RPT; i += 2) {
+                const int r0 = g + CQ_G * i, r1 = r0 + CQ_G;
+                const cplx x0 = xs[p][r0], x1 = xs[p][r1];
+                const bool u0 = !top || r0 >= NB || r0 > j, u1 = !top || r1 >= NB || r1 > j;
+                if (u0) {
+                    s0r = fma(x0.x, a[i].x, fma(x0.y, a[i].y, s0r));
+                    s0i = fma(x0.x, a[i].y, fma(-x0.y, a[i].x, s0i));
                 }
-            } else {
+                if (u1) {
+                    s1r = fma(x1.x, a[i + 1].x, fma(x1.y, a[i + 1].y, s1r));
+                    s1i = fma(x1.x, a[i + 1].y, fma(-x1.y, a[i + 1].x, s1i));
+                }
+            }
+            double sr = s0r + s1r, si = s0i + s1i;
 #pragma unroll
-                for (int i = 0; i < CQ_RPT; ++i) a[i] = csub(a[i], cmul(xs[p][g + CQ_G * i], ef));
+            for (int o = 1; o < CQ_G; o <<= 1) {
+                sr += __shfl_xor_sync(0xffffffffu, sr, o);
+                si += __shfl_xor_sync(0xffffffffu, si, o);
+            }
+            // phase 2: push to every CTA of the cluster (DSMEM stores)
+            if (k >= j) {
+                const cplx part = cmake(sr, si);
+                const cplx pv = top ? pivst[p][k] : cmake(0, 0);
+                for (int d = g; d < C; d += CQ_G) {
+                    cluster.map_shared_rank(&recv[p][rank][0], d)[k] = part;
+                    if (top) cluster.map_shared_rank(&piv[p][0], d)[k] = pv;
+                }
             }
         }
-        if (top) {
-            // diagonal of R, and stage row j+1 for the next pivot broadcast
-#pragma unroll
-            for (int i = 0; i < CQ_RPT / 2; ++i) {   // rows < NB
-                const int r = g + CQ_G * i;
-                if (k == j && r == j) a[i] = diag;
-                if (r == j + 1) pivst[p ^ 1][k] = a[i];
+        cluster.sync();   // release/acquire: publishes the partial sums
+        if (wactive) {
+            // phase 3: the CQ_G lanes of column k split the sources; a fixed
+            // reduction tree keeps every CTA bit-identical
+            cplx Sk = cmake(0, 0), Sj = cmake(0, 0);
+            for (int c = g; c < C; c += CQ_G) {
+                Sk = cadd(Sk, recv[p][c][k]);
+                Sj = cadd(Sj, recv[p][c][j]);
             }
-        }
-        if (k == j + 1) {
 #pragma unroll
-            for (int i = 0; i < CQ_RPT; ++i) xs[p ^ 1][g + CQ_G * i] = a[i];
+            for (int o = 1; o < CQ_G; o <<= 1) {
+                Sk.x += __shfl_xor_sync(0xffffffffu, Sk.x, o);
+                Sk.y += __shfl_xor_sync(0xffffffffu, Sk.y, o);
+                Sj.x += __shfl_xor_sync(0xffffffffu, Sj.x, o);
+            }
+            const double xnorm2 = Sj.x;
+            const cplx alpha = piv[p][j];
+            const cplx pk = piv[p][k];
+            cplx t = cmake(0, 0), scale = cmake(1, 0), diag = alpha;
+            const bool reflect = !(xnorm2 == 0.0 && alpha.y == 0.0);
+            if (reflect) {
+                const double beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xnorm2), alpha.x);
+                const cplx den = cmake(alpha.x - beta, alpha.y);
+                const double ib = 1.0 / beta;
+                const double idd = 1.0 / (den.x * den.x + den.y * den.y);
+                t = cmake((beta - alpha.x) * ib, -alpha.y * ib);
+                scale = cmake(den.x * idd, -den.y * idd);
+                diag = cmake(beta, 0);
+            }
+            if (k == j && g == 0) {
+                colscale[j] = scale;
+                taus[j] = t;
+            }
+            // phase 4: apply H_j^H = I - conj(tau) v v^H to the trailing columns
+            if (reflect && k > j && k < nb) {
+                const cplx cf = cmul(cconj(t), cadd(pk, cmul(cconj(scale), Sk)));
+                const cplx ef = cmul(scale, cf);
+                if (top) {
+#pragma unroll
+                    for (int i = 0; i < CQ_RPT; ++i) {
+                        const int r = g + CQ_G * i;
+                        if (r < NB && r == j) a[i] = csub(a[i], cf);
+                        else if (r >= NB || r > j) a[i] = csub(a[i], cmul(xs[p][r], ef));
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < CQ_RPT; ++i) a[i] = csub(a[i], cmul(xs[p][g + CQ_G * i], ef));
+                }
+            }
+            if (top && k >= j) {
+                // diagonal of R, and stage row j+1 for the next pivot broadcast
+#pragma unroll
+                for (int i = 0; i < CQ_RPT / 2; ++i) {   // rows < NB
+                    const int r = g + CQ_G * i;
+                    if (k == j && r == j) a[i] = diag;
+                    if (r == j + 1) pivst[p ^ 1][k] = a[i];
+                }
+            }
+            if (k == j + 1) {
+#pragma unroll
+                for (int i = 0; i < CQ_RPT; ++i) xs[p ^ 1][g + CQ_G * i] = a[i];
+            }
         }
         __syncthreads();
     }
@@ -490,7 +492,7 @@ bool cluster_qr_available() {
 }
 
 void launch_cluster_block(Context& ctx, int mp, int nb, cplx* A, long long lda, cplx* V, long long ldv,
-                          cplx* tau, cplx* G) {
+                          cplx* tau) {
     const int C = std::max(1, std::min(CQ_MAXC, (mp + CQ_MAXR - 1) / CQ_MAXR));
     const int rows = (mp + C - 1) / C;
     cudaLaunchConfig_t cfg = {};
@@ -504,7 +506,7 @@ void launch_cluster_block(Context& ctx, int mp, int nb, cplx* A, long long lda, 
     at[0].val.clusterDim.z = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    NC_CUDA(cudaLaunchKernelEx(&cfg, cluster_block_qr_kernel, mp, nb, rows, A, lda, V, ldv, tau, G));
+    NC_CUDA(cudaLaunchKernelEx(&cfg, cluster_block_qr_kernel, mp, nb, rows, A, lda, V, ldv, tau));
     ctx.launches++;
 }
 
@@ -568,7 +570,8 @@ void householder_qr(Context& ctx, int m, int n, cplx* A, cplx* Q, cplx* R, bool 
         const cplx* Vb = V + j0 + j0 * (long long)m;
         cplx* T = Tb + (size_t)ob * NB * NB;
         if (use_cluster) {
-            launch_cluster_block(ctx, mp, nb, A + j0 + j0 * lda, lda, V + j0 + j0 * (long long)m, m, tau + j0, G);
+            launch_cluster_block(ctx, mp, nb, A + j0 + j0 * lda, lda, V + j0 + j0 * (long long)m, m, tau + j0);
+            zgemm(zgemm_params(OP_C, OP_N, nb, nb, mp, Vb, m, Vb, m, G, nb), ctx);
         } else {
             for (int jj = j0; jj < j0 + nb; jj += JB) {
                 const int jb = std::min(JB, j0 + nb - jj);
