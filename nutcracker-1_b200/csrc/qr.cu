@@ -225,60 +225,72 @@ __global__ void __launch_bounds__(PT) panel_apply_kernel(int mp, int jb, const c
     }
 }
 
-// Compact-WY T (nb x nb, zlarft forward/columnwise) from the strict upper
-// part of G = V^H V and tau:  T(j,j) = tau_j,
-// T(0:j,j) = -tau_j T(0:j,0:j) G(0:j,j).
-// One CTA; row i of T is owned by a quad of lanes (lane q holds T(i,l) for
-// l = q mod 4 in registers), so the columns are produced without any block
-// barrier: each step is a <= 16-term dot per lane and a quad reduction.
-__global__ void __launch_bounds__(4 * NB) build_t_kernel(int nb, const cplx* __restrict__ G,
-                                                        const cplx* __restrict__ tau, cplx* __restrict__ T,
-                                                        int ldt) {
-    __shared__ cplx Gp[NB * (NB - 1) / 2];   // column j at j(j-1)/2, rows 0..j-1
-    __shared__ cplx taus[NB];
-    for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-        const int l = e % nb, j = e / nb;
-        if (l < j) Gp[j * (j - 1) / 2 + l] = G[e];
+// Compact-WY T (nb x nb, forward/columnwise: H_0 H_1 ... = I - V T V^H) from
+// the strict upper part of G = V^H V and tau, by recursive doubling: with T
+// known on two adjacent diagonal blocks a, b of size s,
+//   T(a,b) = -T(a,a) G(a,b) T(b,b)
+// (the block form of the zlarft recurrence; Puglisi 1992, Joffrain et al.
+// 2006), so six levels of small block products build the 64 x 64 T.  One
+// CTA, T, G and the level's products in shared memory.
+constexpr int BT_T = 256;
+constexpr size_t BT_SMEM = sizeof(cplx) * ((size_t)2 * NB * (NB + 1) + NB * NB / 2);
+
+__global__ void __launch_bounds__(BT_T) build_t_kernel(int nb, const cplx* __restrict__ G,
+                                                      const cplx* __restrict__ tau, cplx* __restrict__ T,
+                                                      int ldt) {
+    extern __shared__ __align__(16) unsigned char bt_smem[];
+    cplx* Ts = reinterpret_cast<cplx*>(bt_smem);   // [NB][NB+1]
+    cplx* Gs = Ts + NB * (NB + 1);                   // [NB][NB+1], strict upper part
+    cplx* Xs = Gs + NB * (NB + 1);                   // one level's G(a,b) T(b,b) blocks
+    const int tid = threadIdx.x;
+    for (int e = tid; e < NB * NB; e += BT_T) {
+        const int i = e % NB, j = e / NB;
+        Gs[i * (NB + 1) + j] = (i < j && j < nb) ? G[i + (long long)nb * j] : cmake(0, 0);
+        Ts[i * (NB + 1) + j] = (i == j && i < nb) ? tau[i] : cmake(0, 0);
     }
-    for (int e = threadIdx.x; e < NB; e += blockDim.x) taus[e] = (e < nb) ? tau[e] : cmake(0, 0);
     __syncthreads();
-    const int i = threadIdx.x >> 2, q = threadIdx.x & 3;
-    cplx t[NB / 4];
-#pragma unroll
-    for (int m = 0; m < NB / 4; ++m) t[m] = cmake(0, 0);
-#pragma unroll
-    for (int jm = 0; jm < NB / 4; ++jm) {
-#pragma unroll
-        for (int jq = 0; jq < 4; ++jq) {
-            const int j = 4 * jm + jq;
-            if (j >= nb) break;
-            // partial sum over l = q + 4m, i <= l < j
-            double sr = 0, si = 0;
-#pragma unroll
-            for (int m = 0; m <= jm; ++m) {
-                const int l = q + 4 * m;
-                if (l < j && l >= i) {
-                    const cplx gv = Gp[j * (j - 1) / 2 + l];
-                    sr = fma(t[m].x, gv.x, fma(-t[m].y, gv.y, sr));
-                    si = fma(t[m].x, gv.y, fma(t[m].y, gv.x, si));
-                }
+    for (int s = 1; s < NB; s <<= 1) {
+        const int per = s * s, total = (NB / (2 * s)) * per;
+        for (int e = tid; e < total; e += BT_T) {   // X = G(a,b) T(b,b), T(b,b) upper
+            const int pr = e / per, rem = e % per, i = rem / s, j = rem % s;
+            const int a0 = 2 * pr * s, b0 = a0 + s;
+            double xr = 0, xi = 0;
+            for (int l = 0; l <= j; ++l) {
+                const cplx g = Gs[(a0 + i) * (NB + 1) + b0 + l], t = Ts[(b0 + l) * (NB + 1) + b0 + j];
+                xr = fma(g.x, t.x, fma(-g.y, t.y, xr));
+                xi = fma(g.x, t.y, fma(g.y, t.x, xi));
             }
-            sr += __shfl_xor_sync(0xffffffffu, sr, 1);
-            si += __shfl_xor_sync(0xffffffffu, si, 1);
-            sr += __shfl_xor_sync(0xffffffffu, sr, 2);
-            si += __shfl_xor_sync(0xffffffffu, si, 2);
-            const cplx tj = taus[j];
-            cplx v = cmake(0, 0);
-            if (i < j) v = cscale(cmul(tj, cmake(sr, si)), -1.0);
-            else if (i == j) v = tj;
-            if (q == jq) t[jm] = v;
+            Xs[e] = cmake(xr, xi);
         }
+        __syncthreads();
+        for (int e = tid; e < total; e += BT_T) {   // T(a,b) = -T(a,a) X, T(a,a) upper
+            const int pr = e / per, rem = e % per, i = rem / s, j = rem % s;
+            const int a0 = 2 * pr * s, b0 = a0 + s;
+            double tr = 0, ti = 0;
+            for (int l = i; l < s; ++l) {
+                const cplx t = Ts[(a0 + i) * (NB + 1) + a0 + l], x = Xs[pr * per + l * s + j];
+                tr = fma(t.x, x.x, fma(-t.y, x.y, tr));
+                ti = fma(t.x, x.y, fma(t.y, x.x, ti));
+            }
+            Ts[(a0 + i) * (NB + 1) + b0 + j] = cmake(-tr, -ti);
+        }
+        __syncthreads();
     }
-#pragma unroll
-    for (int m = 0; m < NB / 4; ++m) {
-        const int l = q + 4 * m;
-        T[i + (long long)ldt * l] = (i < nb && l < nb) ? t[m] : cmake(0, 0);
+    for (int e = tid; e < NB * NB; e += BT_T) {
+        const int i = e % NB, j = e / NB;
+        T[i + (long long)ldt * j] = Ts[i * (NB + 1) + j];
     }
+}
+
+void launch_build_t(Context& ctx, int nb, const cplx* G, const cplx* tau, cplx* T) {
+    static bool attr = false;
+    if (!attr) {
+        NC_CUDA(cudaFuncSetAttribute(build_t_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BT_SMEM));
+        attr = true;
+    }
+    build_t_kernel<<<1, BT_T, BT_SMEM, ctx.stream>>>(nb, G, tau, T, NB);
+    NC_CHECK_LAUNCH();
+    ctx.launches++;
 }
 
 // ---------------------------------------------------------------------------
@@ -588,9 +600,7 @@ void householder_qr(Context& ctx, int m, int n, cplx* A, cplx* Q, cplx* R, bool 
             zgemm(zgemm_params(OP_C, OP_N, nb, nb, mp, Vb, m, Vb, m, G, nb), ctx);
         }
         // compact WY T for the outer block from G = V^H V (strict upper part)
-        build_t_kernel<<<1, 4 * NB, 0, ctx.stream>>>(nb, G, tau + j0, T, NB);
-        NC_CHECK_LAUNCH();
-        ctx.launches++;
+        launch_build_t(ctx, nb, G, tau + j0, T);
         // trailing update: A2 -= V T^H (V^H A2)
         const int nt = n - (j0 + nb);
         if (nt > 0) {
@@ -631,6 +641,96 @@ void householder_qr(Context& ctx, int m, int n, cplx* A, cplx* Q, cplx* R, bool 
     }
 }
 
+// Look-ahead form of householder_qr for the gauge moves (cluster path only).
+// The main stream (ctx) runs the critical path: factor block k, build T_k,
+// then apply reflector k to block k+1 only, so that block k+1 can be
+// factorised next.  The side stream applies reflector k to the remaining
+// columns and accumulates Q forwards, Q <- Q (I - V_k T_k V_k^H) on an m x m
+// Q, while the main stream factors the following blocks on the cluster's
+// 16 SMs.  Forward accumulation costs about twice the flops of the backward
+// order but overlaps the panels instead of following them.  ev: 2 + 2*nblocks
+// events (fork, join, then per block: T_k ready, bulk update k done).
+void householder_qr_lookahead(Context& ctx, Context& side, cudaEvent_t* ev, int m, int n, cplx* A, cplx* Q,
+                              cplx* R, bool conjR) {
+    NC_ARG(m >= n && n >= 1 && m <= CQ_MAXC * CQ_MAXR, "householder_qr: need 1 <= n <= m <= 2048");
+    Arena& ar = ctx.scratch();
+    ArenaFrame f(ar);
+    const long long lda = m;
+    const int nblocks = (n + NB - 1) / NB;
+    cplx* V = ar.alloc_n<cplx>((size_t)m * n);
+    cplx* tau = ar.alloc_n<cplx>(n);
+    cplx* Tb = ar.alloc_n<cplx>((size_t)nblocks * NB * NB);
+    cplx* G = ar.alloc_n<cplx>(NB * NB);
+    cplx* Wm = ar.alloc_n<cplx>(NB * NB);
+    cplx* W2m = ar.alloc_n<cplx>(NB * NB);
+    cplx* Ws = ar.alloc_n<cplx>((size_t)NB * n);
+    cplx* W2s = ar.alloc_n<cplx>((size_t)NB * n);
+    cplx* QW = ar.alloc_n<cplx>((size_t)m * NB);
+    cplx* QW2 = ar.alloc_n<cplx>((size_t)m * NB);
+    cplx* Qf = ar.alloc_n<cplx>((size_t)m * m);
+    const uint64_t side0 = side.launches;
+
+    NC_CUDA(cudaEventRecord(ev[0], ctx.stream));   // fork
+    NC_CUDA(cudaStreamWaitEvent(side.stream, ev[0], 0));
+    identity_cols<<<gsz((long long)m * m), 256, 0, side.stream>>>(m, m, Qf);
+    NC_CHECK_LAUNCH();
+    side.launches++;
+    for (int ob = 0; ob < nblocks; ++ob) {
+        const int j0 = ob * NB, nb = std::min(NB, n - j0), mp = m - j0;
+        const cplx* Vb = V + j0 + j0 * (long long)m;
+        cplx* T = Tb + (size_t)ob * NB * NB;
+        cudaEvent_t ev_t = ev[2 + 2 * ob], ev_bulk = ev[3 + 2 * ob];
+        // main: factor block ob, then T_ob
+        launch_cluster_block(ctx, mp, nb, A + j0 + j0 * lda, lda, V + j0 + j0 * (long long)m, m, tau + j0);
+        zgemm(zgemm_params(OP_C, OP_N, nb, nb, mp, Vb, m, Vb, m, G, nb), ctx);
+        launch_build_t(ctx, nb, G, tau + j0, T);
+        NC_CUDA(cudaEventRecord(ev_t, ctx.stream));
+        const int j1 = j0 + nb, nb1 = (ob + 1 < nblocks) ? std::min(NB, n - j1) : 0;
+        if (nb1 > 0) {
+            // main: reflector ob on block ob+1, after the side stream's update of
+            // those columns by reflector ob-1
+            if (ob > 0) NC_CUDA(cudaStreamWaitEvent(ctx.stream, ev[3 + 2 * (ob - 1)], 0));
+            cplx* A1 = A + j0 + j1 * lda;
+            zgemm(zgemm_params(OP_C, OP_N, nb, nb1, mp, Vb, m, A1, lda, Wm, nb), ctx);
+            zgemm(zgemm_params(OP_C, OP_N, nb, nb1, nb, T, NB, Wm, nb, W2m, nb), ctx);
+            ZGemmParams p = zgemm_params(OP_N, OP_N, mp, nb1, nb, Vb, m, W2m, nb, A1, lda);
+            p.alpha = cmake(-1, 0);
+            p.beta = cmake(1, 0);
+            zgemm(p, ctx);
+        }
+        // side: reflector ob on the columns after block ob+1, then Q
+        NC_CUDA(cudaStreamWaitEvent(side.stream, ev_t, 0));
+        const int jr = j1 + nb1, nt = n - jr;
+        if (nt > 0) {
+            cplx* A2 = A + j0 + jr * lda;
+            zgemm(zgemm_params(OP_C, OP_N, nb, nt, mp, Vb, m, A2, lda, Ws, nb), side);
+            zgemm(zgemm_params(OP_C, OP_N, nb, nt, nb, T, NB, Ws, nb, W2s, nb), side);
+            ZGemmParams p = zgemm_params(OP_N, OP_N, mp, nt, nb, Vb, m, W2s, nb, A2, lda);
+            p.alpha = cmake(-1, 0);
+            p.beta = cmake(1, 0);
+            zgemm(p, side);
+        }
+        NC_CUDA(cudaEventRecord(ev_bulk, side.stream));
+        // Qf(:, j0:) -= (Qf(:, j0:) V_ob) T_ob V_ob^H
+        cplx* Qs = Qf + j0 * (long long)m;
+        zgemm(zgemm_params(OP_N, OP_N, m, nb, mp, Qs, m, Vb, m, QW, m), side);
+        zgemm(zgemm_params(OP_N, OP_N, m, nb, nb, QW, m, T, NB, QW2, m), side);
+        ZGemmParams q = zgemm_params(OP_N, OP_C, m, mp, nb, QW2, m, Vb, m, Qs, m);
+        q.alpha = cmake(-1, 0);
+        q.beta = cmake(1, 0);
+        zgemm(q, side);
+    }
+    NC_CUDA(cudaEventRecord(ev[1], side.stream));   // join
+    NC_CUDA(cudaStreamWaitEvent(ctx.stream, ev[1], 0));
+    ctx.launches += side.launches - side0;
+    if (R) {
+        extract_r<<<gsz((long long)n * n), 256, 0, ctx.stream>>>(n, A, lda, conjR, R);
+        NC_CHECK_LAUNCH();
+        ctx.launches++;
+    }
+    if (Q) NC_CUDA(cudaMemcpyAsync(Q, Qf, sizeof(cplx) * (size_t)m * n, cudaMemcpyDeviceToDevice, ctx.stream));
+}
+
 // ---------------------------------------------------------------------------
 // gauge moves (core.f95:2708-2960 semantics, QR gauge)
 // ---------------------------------------------------------------------------
@@ -644,6 +744,10 @@ struct QrPlan {
     int m = 0, n = 0;
     bool conjR = false;
     Arena arena;
+    // look-ahead: second stream (own context, own split-K arena) and events
+    std::unique_ptr<Context> side;
+    Arena side_arena;
+    std::vector<cudaEvent_t> ev;
     cplx* X = nullptr;   // input (m x n), overwritten
     cplx* Q = nullptr;   // explicit Q (m x n)
     cplx* R = nullptr;   // R (n x n), conjugated if conjR
@@ -653,6 +757,7 @@ struct QrPlan {
     ~QrPlan() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
     }
 };
 
@@ -666,6 +771,12 @@ QrPlan& qr_plan(Context& ctx, int m, int n, bool conjR) {
     p->X = p->arena.alloc_n<cplx>((size_t)m * n);
     p->Q = p->arena.alloc_n<cplx>((size_t)m * n);
     p->R = p->arena.alloc_n<cplx>((size_t)n * n);
+    if (cluster_qr_available()) {
+        p->side = std::make_unique<Context>();
+        p->side->ws_override = &p->side_arena;
+        p->ev.resize(2 + 2 * ((n + NB - 1) / NB));
+        for (cudaEvent_t& e : p->ev) NC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
     plans.push_back(std::move(p));
     return *plans.back();
 }
@@ -681,12 +792,16 @@ void qr_run(Context& ctx, QrPlan& P) {
     const bool prof = ctx.profile;
     ctx.profile = false;
     ctx.ws_override = &P.arena;
+    auto once = [&] {
+        if (P.side) householder_qr_lookahead(ctx, *P.side, P.ev.data(), P.m, P.n, P.X, P.Q, P.R, P.conjR);
+        else householder_qr(ctx, P.m, P.n, P.X, P.Q, P.R, P.conjR);
+    };
     try {
-        householder_qr(ctx, P.m, P.n, P.X, P.Q, P.R, P.conjR);
+        once();
         const uint64_t l0 = ctx.launches;
         NC_CUDA(cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeRelaxed));
         try {
-            householder_qr(ctx, P.m, P.n, P.X, P.Q, P.R, P.conjR);
+            once();
         } catch (...) {
             cudaGraph_t g = nullptr;
             cudaStreamEndCapture(ctx.stream, &g);
