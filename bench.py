@@ -70,6 +70,14 @@ def parse():
                     help="both (default): time FP64 and precision-form sweeps from the same state; "
                          "value is the precision form's")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving-loop sample")
+    ap.add_argument("--serving-only", action="store_true", help="run only the serving-loop sample")
+    ap.add_argument("--serve-requests", type=int, default=48,
+                    help="requests in the serving sample (the serving workload has 20k; a bounded sample)")
+    ap.add_argument("--serve-plain", type=int, default=8,
+                    help="requests of the same stream timed one at a time (the plain per-solve baseline)")
+    ap.add_argument("--serve-slots", type=int, default=0, help="concurrent requests (0: min(16, cores - 2))")
+    ap.add_argument("--serve-rate", type=float, default=64.0, help="Poisson arrival rate, requests/s")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--phases", action="store_true",
                     help="synchronise and time each sweep phase (diagnostics; slows the sweep slightly)")
@@ -77,6 +85,9 @@ def parse():
                     help="time only the Householder-QR gauge move of a chi x chi site (kernel profiling)")
     ap.add_argument("--heff-only", action="store_true",
                     help="time only the effective-Hamiltonian product at --chi (kernel profiling)")
+    ap.add_argument("--tc-gemm-only", action="store_true",
+                    help="time only the tcgen05 3xTF32 complex GEMM of the stage-A shape at --chi "
+                         "(M=chi, N=5*chi, K=chi; kernel profiling)")
     return ap.parse_args()
 
 
@@ -124,6 +135,124 @@ def run_heff_only(args):
     t = e0.elapsed_time(e1) / 1e3 / args.steps
     flops = 8 * d * chi * chi * (cl * chi + cr * chi) + 8 * op.nnz * d * d * chi * chi
     print(json.dumps({"heff_chi": chi, "ms": t * 1e3, "tflops": flops / t / 1e12}), flush=True)
+
+
+def run_tc_gemm_only(args):
+    """W + K calls of the tcgen05 3xTF32 complex GEMM on the stage-A shape of
+    the chi x chi interior site (psi_a times the five left-environment blocks),
+    seeded random complex128 operands, through nc_tc_zgemm_dev."""
+    import ctypes as ct
+    import torch
+
+    import nutcracker_b200 as nb
+
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    nb.lib.nc_set_stream(ct.c_void_p(stream.cuda_stream))
+    M, N, K = args.chi, 5 * args.chi, args.chi
+    g = torch.Generator(device="cuda").manual_seed(args.seed)
+    A = torch.randn(K, M, dtype=torch.complex128, device="cuda", generator=g)   # column-major M x K
+    B = torch.randn(N, K, dtype=torch.complex128, device="cuda", generator=g)   # column-major K x N
+    C = torch.empty((N, M), dtype=torch.complex128, device="cuda")
+
+    def once():
+        if nb.lib.nc_tc_zgemm_dev(M, N, K, ct.c_void_p(A.data_ptr()), ct.c_void_p(B.data_ptr()),
+                                  ct.c_void_p(C.data_ptr()), 1) != 0:
+            nb._check()
+
+    for _ in range(args.warmup):
+        once()
+    nb.lib.nc_profile_begin(ct.c_double(1e9))
+    for _ in range(args.steps):
+        once()
+    n, ms, fl = ct.c_uint64(), ct.c_double(), ct.c_double()
+    nb.lib.nc_profile_query(1, ct.byref(n), ct.byref(ms), ct.byref(fl))
+    nb.lib.nc_profile_end(ct.byref(ct.c_uint64()), ct.byref(ct.c_double()), ct.byref(ct.c_double()))
+    print(json.dumps({"tc_gemm": [M, N, K], "launches": n.value, "ms_per_launch": ms.value / max(n.value, 1),
+                      "tf32_tflops": fl.value / (ms.value * 1e-3) / 1e12 if ms.value > 0 else None}), flush=True)
+
+
+def serving_sample(args):
+    """Serving workload sample: transverse-field Ising solves H = -sum ZZ - lam sum X with
+    lam ~ U[0.5,1.5], N ~ U{8..128}, chi ~ U{16..256} (capped at the chain's maximum bond
+    dimension), 1-4 levels each, FP64, seeded, Poisson arrivals.  The first `serve_plain`
+    requests are also run one at a time (the plain per-solve throughput); the serving run
+    submits the whole stream on its arrival schedule to a server with several slots."""
+    from nutcracker_b200 import operators
+    from nutcracker_b200.serve import Server
+    from oracle import ed, mpo
+
+    rng = np.random.default_rng(args.seed + 5)
+    reqs = []
+    for _ in range(args.serve_requests):
+        n = int(rng.integers(8, 129))
+        lam = float(rng.uniform(0.5, 1.5))
+        chi = int(min(rng.integers(16, 257), 2 ** (n // 2)))
+        levels = int(rng.integers(1, 5))
+        reqs.append((n, lam, chi, levels))
+    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, size=len(reqs)))
+    ops = {}
+
+    def op(n, lam):
+        if (n, lam) not in ops:
+            ops[(n, lam)] = operators.ferromagnetic_transverse_ising(n, lam)
+        return ops[(n, lam)]
+
+    def submit(srv, r, k):
+        n, lam, chi, levels = r
+        return srv.submit(op(n, lam), levels=levels, initial_bandwidth_dimension=chi, seed=1000 + k)
+
+    slots = args.serve_slots or max(1, min(16, os.cpu_count() or 4))
+    with Server(max_inflight=slots) as srv:
+        # warm every worker (thread context, arena, first QR plans) with small solves
+        warm = operators.ferromagnetic_transverse_ising(16, 1.0)
+        for i in [srv.submit(warm, levels=1, initial_bandwidth_dimension=16, seed=1) for _ in range(slots)]:
+            srv.wait(i)
+        # plain per-solve baseline: the first requests of the stream one at a time
+        plain = []
+        t0 = time.perf_counter()
+        for k, r in enumerate(reqs[:args.serve_plain]):
+            plain.append(srv.wait(submit(srv, r, k)))
+        t_plain = time.perf_counter() - t0
+        # the stream on its arrival schedule
+        start = time.perf_counter()
+        ids = []
+        for k, r in enumerate(reqs):
+            delay = arrivals[k] - (time.perf_counter() - start)
+            if delay > 0:
+                time.sleep(delay)
+            ids.append(submit(srv, r, k))
+        res = [srv.wait(i) for i in ids]
+        window = time.perf_counter() - start
+        after = srv.stats()
+    lat = sorted(x["seconds_total"] for x in res if x["status"] == 0)
+    pct = (lambda q: lat[min(len(lat) - 1, int(np.ceil(q * len(lat))) - 1)]) if lat else (lambda q: None)
+    st = {"solves_per_second": len(lat) / window if window > 0 else None, "p50_seconds": pct(0.5),
+          "p99_seconds": pct(0.99), "mean_seconds": float(np.mean(lat)) if lat else None,
+          "window_seconds": window, "peak_bytes_in_flight": after["peak_bytes_in_flight"]}
+    failed = [i for i, x in enumerate(res) if x["status"] != 0]
+    same = max((abs(a - b) / max(abs(a), 1e-300) for p, m in zip(plain, res) for a, b in
+                zip(p["energies"], m["energies"])), default=0.0)
+    ed_err = []
+    for r, x in zip(reqs, res):
+        n, lam, chi, levels = r
+        if n <= 12 and x["status"] == 0:
+            w, _ = ed.lowest_levels(mpo.transverse_ising_ferro(n, lam), levels)
+            ed_err.append(max(abs(e - ref) / n for e, ref in zip(x["energies"], w)))
+    plain_rate = len(plain) / t_plain if t_plain > 0 else None
+    return {
+        "workload": "TFIM -ZZ - lam X: lam~U[0.5,1.5], N~U{8..128}, chi~U{16..256} (<= chain maximum), "
+                    "1-4 levels, FP64, Poisson arrivals at %.0f/s; %d requests (bounded sample of the "
+                    "20k-request stream)" % (args.serve_rate, len(reqs)),
+        "slots": slots, "requests": len(reqs), "failed": len(failed),
+        "solves_per_s": st["solves_per_second"], "p50_s": st["p50_seconds"], "p99_s": st["p99_seconds"],
+        "mean_s": st["mean_seconds"], "window_s": st["window_seconds"],
+        "peak_gb_in_flight": st["peak_bytes_in_flight"] / 1e9,
+        "plain_solves_per_s": plain_rate, "plain_requests": len(plain),
+        "speedup_vs_plain": (st["solves_per_second"] / plain_rate) if plain_rate else None,
+        "max_rel_diff_alone_vs_mix": same,
+        "ed_checked": len(ed_err), "max_dE_per_site_vs_ed": max(ed_err) if ed_err else None,
+    }
 
 
 def run_gauge_only(args):
@@ -510,6 +639,8 @@ def run_ours(args, rank, world):
         line.update({"value": line["fp64"]["value"], "ms_per_step": line["fp64"]["ms_per_step"],
                      "dtype": "complex128", "gpu_launches": line["fp64"]["gpu_launches"],
                      "roofline": line["fp64"]["roofline"], "chain": line["fp64"]["chain"]})
+    if world == 1 and not args.no_serving:
+        line["serving"] = serving_sample(args)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.sites, args.chi)
     print(json.dumps(line), flush=True)
@@ -529,6 +660,12 @@ def main():
     try:
         if args.heff_only:
             run_heff_only(args)
+        elif args.tc_gemm_only:
+            run_tc_gemm_only(args)
+        elif args.serving_only:
+            import torch
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+            print(json.dumps({"serving": serving_sample(args)}), flush=True)
         elif args.gauge_only:
             run_gauge_only(args)
         elif args.impl == "reference":

@@ -360,6 +360,17 @@ int nc_chain_optimize_site(nc_chain* chain);                 /* base_chain.cpp:8
 int nc_chain_perform_optimization_sweep(nc_chain* chain);    /* chain.cpp:147-163 */
 int nc_chain_sweep_until_converged(nc_chain* chain);         /* base_chain.cpp:112-123 */
 int nc_chain_optimize_chain(nc_chain* chain);                /* base_chain.cpp:64-79 */
+/* No counterpart in the reference: `n` levels at the chain's current bond
+   dimension (sweepUntilConverged per level, then the level becomes a
+   projector and the chain resets, as solveForMultipleLevels does around
+   optimizeChain, chain.cpp:301-310, but without bond growth).  energies
+   receives n values. */
+int nc_chain_solve_levels_at_bandwidth(nc_chain* chain, uint32_t n, double* energies);
+/* No counterpart in the reference: estimated device bytes of a chain of this
+   operator at options->initial_bandwidth_dimension for `levels` levels
+   (buffers, solver scratch, gauge plans, 25% margin); host-only. */
+int nc_chain_footprint_bytes(uint32_t number_of_sites, const nc_operator_site* sites,
+                             const nc_chain_options* options, uint32_t levels, uint64_t* bytes);
 /* No counterpart in the reference: switch the precision of the following
    sweeps (0 FP64, 1 precision form).  Going back to FP64 rebuilds every
    environment in FP64 and resets the energy to the FP64 expectation value
@@ -375,6 +386,56 @@ int nc_chain_compute_expectation_value(nc_chain* chain, double* value);
 int nc_chain_get_info(nc_chain* chain, nc_chain_info* info);
 /* Copies site i to host `out` (may be NULL) and writes dims (br,bl,d). */
 int nc_chain_get_site(nc_chain* chain, uint32_t i, nc_complex* out, uint32_t* dims);
+
+/* ---- Serving loop (no counterpart in the reference) ---------------------
+
+   Continuous batching of independent MPO solves on one GPU.  Requests wait
+   in arrival order; a pool of worker threads, each with its own stream and
+   device arena, starts the request at the head of the queue as soon as a
+   worker is free and the request's estimated footprint
+   (nc_chain_footprint_bytes) fits in the memory budget beside the requests
+   already running (a request larger than the budget runs alone).  Each
+   request keeps its MPS and environments on the device for all of its
+   sweeps, solves `levels` levels at options->initial_bandwidth_dimension
+   (nc_chain_solve_levels_at_bandwidth) and releases its memory without
+   synchronising the device.  Results depend only on the request's own
+   inputs, so they are the same alone and in the mix. */
+#define NC_SERVER_MAX_LEVELS 8
+typedef struct {
+    uint32_t max_inflight;          /* worker threads = requests running at once (default 16) */
+    uint64_t memory_budget_bytes;   /* 0: 80% of the device memory free at creation */
+} nc_server_options;
+typedef struct {
+    int32_t status;                 /* 0 or the failing call's status code */
+    uint32_t levels, bandwidth_dimension;
+    double energies[NC_SERVER_MAX_LEVELS];
+    double seconds_queued, seconds_run, seconds_total;   /* submit -> start -> done */
+    uint64_t footprint_bytes, sweeps;
+    char message[128];              /* error message when status != 0 */
+} nc_request_result;
+typedef struct {
+    uint64_t submitted, completed, failed, in_flight, queued;
+    double p50_seconds, p99_seconds, mean_seconds;       /* time to converged (submit -> done) */
+    double solves_per_second, window_seconds;            /* completed / (first submit -> last done) */
+    uint64_t peak_bytes_in_flight, memory_budget_bytes;
+} nc_server_stats;
+typedef struct nc_server nc_server;
+
+void nc_server_options_init(nc_server_options* options);
+/* Starts the worker threads on the current device.  NULL on error. */
+nc_server* nc_server_create(const nc_server_options* options);
+/* Copies the operator and options; returns the request id (> 0) or -1. */
+int64_t nc_server_submit(nc_server* server, uint32_t number_of_sites, const nc_operator_site* sites,
+                         const nc_chain_options* options, uint32_t levels);
+/* 0 and the result when done, 1 while queued or running, else an error. */
+int nc_server_poll(nc_server* server, int64_t id, nc_request_result* result);
+/* Blocks until the request is done. */
+int nc_server_wait(nc_server* server, int64_t id, nc_request_result* result);
+/* Blocks until no request is queued or running. */
+int nc_server_drain(nc_server* server);
+int nc_server_get_stats(nc_server* server, nc_server_stats* stats);
+/* Finishes the queued requests, stops the workers and frees the server. */
+void nc_server_free(nc_server* server);
 
 #ifdef __cplusplus
 }

@@ -25,39 +25,59 @@ namespace nc {
 
 namespace {
 
+// Device buffer in stream-ordered memory (cudaMallocAsync / cudaFreeAsync on
+// the allocating thread's stream): freeing a chain never synchronises the
+// whole device, so chains run by other threads (the serving loop) keep going.
+void keep_pool_memory() {
+    static bool done = false;
+    if (done) return;
+    int dev = 0;
+    cudaMemPool_t pool;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;   // freed blocks stay in this process's pool
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
+    done = true;
+}
+
 struct DevBuf {
     cplx* p = nullptr;
     size_t n = 0;
+    cudaStream_t s = nullptr;
     DevBuf() {}
     explicit DevBuf(size_t count) { alloc(count); }
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
-    DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n), s(o.s) { o.p = nullptr; o.n = 0; }
     DevBuf& operator=(DevBuf&& o) noexcept {
-        if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+        if (this != &o) { release(); p = o.p; n = o.n; s = o.s; o.p = nullptr; o.n = 0; }
         return *this;
     }
     ~DevBuf() { release(); }
     void alloc(size_t count) {
         release();
+        keep_pool_memory();
         if (count == 0) count = 1;
-        cudaError_t e = cudaMalloc(&p, count * sizeof(cplx));
+        s = Context::get().stream;
+        cudaError_t e = cudaMallocAsync(&p, count * sizeof(cplx), s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);   // usable from any stream and the host from here on
         if (e != cudaSuccess) {
             cudaGetLastError();
             p = nullptr;
-            throw Error(NC_ERR_NOMEM, "chain: cudaMalloc of " + std::to_string(count * sizeof(cplx)) + " bytes failed");
+            throw Error(NC_ERR_NOMEM, "chain: allocation of " + std::to_string(count * sizeof(cplx)) + " bytes failed");
         }
         n = count;
     }
     void ensure(size_t count) { if (n < count) alloc(count); }
-    void release() { if (p) cudaFree(p); p = nullptr; n = 0; }
+    void release() { if (p) cudaFreeAsync(p, s); p = nullptr; n = 0; }
 };
 
 struct OpSite {
     MpoSite dev;
     DevBuf W;
+    DevBuf idxbuf;   // (2,nnz) uint32 indices
     uint32_t* idx = nullptr;
-    ~OpSite() { if (idx) cudaFree(idx); }
 };
 
 struct ProjSite {
@@ -121,6 +141,9 @@ struct Chain {
     DevBuf mixbuf;       // MixedHeff operands of the current site (float storage)
     MixedHeff mh;
 
+    // Work on this chain's stream finishes before its buffers return to the pool.
+    ~Chain() { cudaStreamSynchronize(ctx.stream); }
+
     Chain(Context& c, int n, const OperatorSiteDesc* sites, const ChainOptions& o) : ctx(c), opt(o), N(n) {
         NC_ARG(N >= 1, "chain needs at least one site");
         for (int i = 0; i < N; ++i) {
@@ -133,7 +156,8 @@ struct Chain {
             if (i > 0) NC_ARG(sites[i - 1].cr == s.cl, "operator bond dimensions do not connect");
             auto op = std::make_unique<OpSite>();
             op->W.alloc((size_t)s.d * s.d * s.nnz);
-            NC_CUDA(cudaMalloc(&op->idx, 2 * s.nnz * sizeof(uint32_t)));
+            op->idxbuf.alloc((2 * s.nnz * sizeof(uint32_t) + sizeof(cplx) - 1) / sizeof(cplx));
+            op->idx = reinterpret_cast<uint32_t*>(op->idxbuf.p);
             NC_CUDA(cudaMemcpy(op->W.p, s.W, (size_t)s.d * s.d * s.nnz * sizeof(cplx), cudaMemcpyHostToDevice));
             NC_CUDA(cudaMemcpy(op->idx, s.idx, 2 * s.nnz * sizeof(uint32_t), cudaMemcpyHostToDevice));
             op->dev.d = (int)s.d; op->dev.cl = (int)s.cl; op->dev.cr = (int)s.cr; op->dev.nnz = (int)s.nnz;
@@ -650,6 +674,54 @@ struct Chain {
         optimize_chain();
         if (energies) energies[n - 1] = energy;
     }
+
+    // n levels at the current bond dimension: sweepUntilConverged per level
+    // (solve_for_multiple_levels with optimize_chain replaced; no chi growth).
+    void solve_levels_at_bandwidth(int n, double* energies) {
+        for (int k = 0; k < n; ++k) {
+            if (k > 0) {
+                construct_and_add_projector_from_state();
+                reset();
+            }
+            sweep_until_converged();
+            if (energies) energies[k] = energy;
+        }
+    }
+
+    // Device bytes a chain of this operator needs at bond dimension
+    // `bandwidth` for `levels` levels: the buffers allocate_for_bonds and the
+    // projector sites hold, plus the solver's arena peak (Lanczos basis,
+    // H_eff scratch, the precision form's tensor-core operands) and the gauge
+    // moves' QR plans, with a 25% margin.
+    static uint64_t footprint_bytes(const std::vector<int>& d, const std::vector<int>& cl, const std::vector<int>& cr,
+                                    int bandwidth, int levels, int krylov, int precision) {
+        const int n = (int)d.size();
+        const int b = std::min(bandwidth, maximum_bandwidth_dimension(d));
+        const std::vector<int> bonds = bandwidth_sequence(std::max(1, b), d);
+        double elems = 0, maxs = 1, maxenv = 1;
+        for (int i = 0; i < n; ++i) {
+            const double site = (double)bonds[i] * bonds[i + 1] * d[i];
+            maxs = std::max(maxs, site);
+            const double env = (double)bonds[i] * bonds[i] * cl[i] + (double)bonds[i + 1] * bonds[i + 1] * cr[i];
+            maxenv = std::max(maxenv, env);
+            elems += env;
+        }
+        elems += (n + 2) * maxs;                                   // sites and spares
+        const int np = std::max(0, levels - 1);
+        for (int i = 0; i < n; ++i)                                // projector sites and overlap environments
+            elems += np * (3.0 * bonds[i] * bonds[i + 1] * d[i] + (double)bonds[i] * bonds[i] +
+                           (double)bonds[i + 1] * bonds[i + 1]);
+        elems += (krylov + 1 + std::max(4, krylov / 3) + 4) * maxs;   // Lanczos basis, restart vectors
+        elems += 2.0 * maxs * 8 + maxenv;                         // H_eff / environment-update scratch
+        double qr = 0;
+        for (int i = 0; i + 1 < n; ++i) {                          // largest gauge QR plan (m x n, Q accumulated m x m)
+            const double m = (double)bonds[i] * d[i], k = bonds[i + 1];
+            qr = std::max(qr, 4.0 * m * k + m * m + 2.0 * k * k);
+        }
+        elems += 2 * qr;
+        if (precision) elems += 3.0 * maxenv + 4.0 * maxs;       // TF32 pairs of environments and sites (float = elems/4)
+        return (uint64_t)(1.25 * elems * sizeof(cplx)) + (64ull << 20);
+    }
 };
 
 }  // namespace nc
@@ -775,6 +847,30 @@ int nc_chain_solve_for_eigenvalues(nc_chain* c, uint32_t n, double* eigenvalues)
     })
 }
 int nc_chain_get_energy(nc_chain* c, double* energy) { NC_CHAIN_CALL(*energy = ch.energy) }
+int nc_chain_solve_levels_at_bandwidth(nc_chain* c, uint32_t n, double* energies) {
+    NC_CHAIN_CALL({
+        NC_ARG(n >= 1, "need at least one level");
+        ch.solve_levels_at_bandwidth((int)n, energies);
+    })
+}
+
+int nc_chain_footprint_bytes(uint32_t number_of_sites, const nc_operator_site* sites, const nc_chain_options* options,
+                             uint32_t levels, uint64_t* bytes) {
+    NC_ABI_BEGIN
+    NC_ARG(number_of_sites >= 1 && sites && bytes, "bad arguments");
+    std::vector<int> d(number_of_sites), cl(number_of_sites), cr(number_of_sites);
+    for (uint32_t i = 0; i < number_of_sites; ++i) {
+        d[i] = (int)sites[i].physical_dimension;
+        cl[i] = (int)sites[i].left_dimension;
+        cr[i] = (int)sites[i].right_dimension;
+        NC_ARG(d[i] >= 1 && cl[i] >= 1 && cr[i] >= 1, "bad operator site");
+    }
+    const ChainOptions o = to_options(options);
+    *bytes = Chain::footprint_bytes(d, cl, cr, (int)std::max<uint32_t>(1, o.initial_bandwidth_dimension),
+                                    (int)std::max<uint32_t>(1, levels), o.krylov_dim, o.precision);
+    NC_ABI_END
+    return g_status;
+}
 int nc_chain_set_precision(nc_chain* c, uint32_t precision) {
     NC_CHAIN_CALL({
         NC_ARG(precision <= 1, "precision must be 0 (FP64) or 1 (mixed)");

@@ -744,10 +744,13 @@ struct QrPlan {
     int m = 0, n = 0;
     bool conjR = false;
     Arena arena;
-    // look-ahead: second stream (own context, own split-K arena) and events
-    std::unique_ptr<Context> side;
+    // look-ahead: the thread's second stream (side_context) with this plan's
+    // split-K arena, and the plan's events
+    bool lookahead = false;
     Arena side_arena;
     std::vector<cudaEvent_t> ev;
+    // single-block shapes are run directly: recording a graph saves nothing
+    bool capture = true;
     cplx* X = nullptr;   // input (m x n), overwritten
     cplx* Q = nullptr;   // explicit Q (m x n)
     cplx* R = nullptr;   // R (n x n), conjugated if conjR
@@ -762,6 +765,13 @@ struct QrPlan {
 };
 
 namespace {
+// Second stream of this host thread for the look-ahead QR (one per thread,
+// shared by the thread's plans, which run one at a time).
+Context& side_context() {
+    thread_local Context* c = new Context();   // lives until process exit, like Context::get()
+    return *c;
+}
+
 QrPlan& qr_plan(Context& ctx, int m, int n, bool conjR) {
     thread_local std::vector<std::unique_ptr<QrPlan>> plans;
     for (auto& p : plans)
@@ -772,11 +782,11 @@ QrPlan& qr_plan(Context& ctx, int m, int n, bool conjR) {
     p->Q = p->arena.alloc_n<cplx>((size_t)m * n);
     p->R = p->arena.alloc_n<cplx>((size_t)n * n);
     if (cluster_qr_available()) {
-        p->side = std::make_unique<Context>();
-        p->side->ws_override = &p->side_arena;
+        p->lookahead = true;
         p->ev.resize(2 + 2 * ((n + NB - 1) / NB));
         for (cudaEvent_t& e : p->ev) NC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
+    p->capture = n > NB;
     plans.push_back(std::move(p));
     return *plans.back();
 }
@@ -792,10 +802,26 @@ void qr_run(Context& ctx, QrPlan& P) {
     const bool prof = ctx.profile;
     ctx.profile = false;
     ctx.ws_override = &P.arena;
+    Context& side = side_context();
+    side.ws_override = &P.side_arena;
     auto once = [&] {
-        if (P.side) householder_qr_lookahead(ctx, *P.side, P.ev.data(), P.m, P.n, P.X, P.Q, P.R, P.conjR);
-        else householder_qr(ctx, P.m, P.n, P.X, P.Q, P.R, P.conjR);
+        if (P.lookahead && P.capture)
+            householder_qr_lookahead(ctx, side, P.ev.data(), P.m, P.n, P.X, P.Q, P.R, P.conjR);
+        else
+            householder_qr(ctx, P.m, P.n, P.X, P.Q, P.R, P.conjR);
     };
+    if (!P.capture) {
+        try {
+            once();
+        } catch (...) {
+            ctx.ws_override = nullptr;
+            ctx.profile = prof;
+            throw;
+        }
+        ctx.ws_override = nullptr;
+        ctx.profile = prof;
+        return;
+    }
     try {
         once();
         const uint64_t l0 = ctx.launches;
