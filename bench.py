@@ -72,8 +72,11 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-loop sample")
     ap.add_argument("--serving-only", action="store_true", help="run only the serving-loop sample")
-    ap.add_argument("--serve-requests", type=int, default=48,
+    ap.add_argument("--serve-requests", type=int, default=32,
                     help="requests in the serving sample (the serving workload has 20k; a bounded sample)")
+    ap.add_argument("--serve-full", action="store_true",
+                    help="draw N and chi from the serving workload's full ranges (N<=128, chi<=256); the "
+                         "default halves them (N<=64, chi<=128) to keep the default run within minutes")
     ap.add_argument("--serve-plain", type=int, default=8,
                     help="requests of the same stream timed one at a time (the plain per-solve baseline)")
     ap.add_argument("--serve-slots", type=int, default=0, help="concurrent requests (0: min(16, cores - 2))")
@@ -184,10 +187,11 @@ def serving_sample(args):
 
     rng = np.random.default_rng(args.seed + 5)
     reqs = []
+    n_hi, chi_hi = (128, 256) if args.serve_full else (64, 128)
     for _ in range(args.serve_requests):
-        n = int(rng.integers(8, 129))
+        n = int(rng.integers(8, n_hi + 1))
         lam = float(rng.uniform(0.5, 1.5))
-        chi = int(min(rng.integers(16, 257), 2 ** (n // 2)))
+        chi = int(min(rng.integers(16, chi_hi + 1), 2 ** (n // 2)))
         levels = int(rng.integers(1, 5))
         reqs.append((n, lam, chi, levels))
     arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, size=len(reqs)))
@@ -241,9 +245,10 @@ def serving_sample(args):
             ed_err.append(max(abs(e - ref) / n for e, ref in zip(x["energies"], w)))
     plain_rate = len(plain) / t_plain if t_plain > 0 else None
     return {
-        "workload": "TFIM -ZZ - lam X: lam~U[0.5,1.5], N~U{8..128}, chi~U{16..256} (<= chain maximum), "
+        "workload": "TFIM -ZZ - lam X: lam~U[0.5,1.5], N~U{8..%d}, chi~U{16..%d} (<= chain maximum), "
                     "1-4 levels, FP64, Poisson arrivals at %.0f/s; %d requests (bounded sample of the "
-                    "20k-request stream)" % (args.serve_rate, len(reqs)),
+                    "20k-request stream%s)" % (n_hi, chi_hi, args.serve_rate, len(reqs),
+                                               "" if args.serve_full else "; N and chi ranges halved"),
         "slots": slots, "requests": len(reqs), "failed": len(failed),
         "solves_per_s": st["solves_per_second"], "p50_s": st["p50_seconds"], "p99_s": st["p99_seconds"],
         "mean_s": st["mean_seconds"], "window_s": st["window_seconds"],

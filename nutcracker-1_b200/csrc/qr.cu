@@ -232,7 +232,7 @@ __global__ void __launch_bounds__(PT) panel_apply_kernel(int mp, int jb, const c
 // (the block form of the zlarft recurrence; Puglisi 1992, Joffrain et al.
 // 2006), so six levels of small block products build the 64 x 64 T.  One
 // CTA, T, G and the level's products in shared memory.
-constexpr int BT_T = 256;
+constexpr int BT_T = 1024;
 constexpr size_t BT_SMEM = sizeof(cplx) * ((size_t)2 * NB * (NB + 1) + NB * NB / 2);
 
 __global__ void __launch_bounds__(BT_T) build_t_kernel(int nb, const cplx* __restrict__ G,
