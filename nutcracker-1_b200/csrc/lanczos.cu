@@ -101,6 +101,127 @@ __global__ void multi_axpy_kernel(long long n, int k, const cplx* __restrict__ V
     }
 }
 
+// One classical Gram-Schmidt pass against V_0..V_{k-1} in one launch:
+// out = w - sum_i hsub_i V_i (hsub may be null: out is not written), then
+// h = V^H out over the updated vector.  Blocks (x: elements, y: chunks of KC
+// vectors) store partial sums; the last block to finish adds them in block
+// order (fixed, so the result does not depend on block timing).  Every chunk
+// forms the updated vector itself; chunk 0 writes it.
+__global__ void __launch_bounds__(RT) cgs_pass_kernel(long long n, int k, const cplx* __restrict__ V,
+                                                      const cplx* __restrict__ w, const cplx* __restrict__ hsub,
+                                                      cplx* __restrict__ out, cplx* __restrict__ part,
+                                                      unsigned* __restrict__ counter, cplx* __restrict__ h) {
+    __shared__ cplx hs[MAXM];
+    __shared__ double sr[KC][RT / 32], si[KC][RT / 32];
+    __shared__ bool last;
+    if (hsub)
+        for (int i = threadIdx.x; i < k; i += blockDim.x) hs[i] = hsub[i];
+    __syncthreads();
+    const int c0 = blockIdx.y * KC;
+    const int kc = min(KC, k - c0);
+    double ar[KC], ai[KC];
+#pragma unroll
+    for (int i = 0; i < KC; ++i) ar[i] = ai[i] = 0;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+         e += (long long)gridDim.x * blockDim.x) {
+        cplx b = w[e];
+        if (hsub) {
+            for (int i = 0; i < k; ++i) b = csub(b, cmul(hs[i], V[(size_t)i * n + e]));
+            if (blockIdx.y == 0) out[e] = b;
+        }
+#pragma unroll
+        for (int i = 0; i < KC; ++i) {
+            if (i < kc) {
+                const cplx a = V[(size_t)(c0 + i) * n + e];
+                ar[i] += a.x * b.x + a.y * b.y;
+                ai[i] += a.x * b.y - a.y * b.x;
+            }
+        }
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int i = 0; i < KC; ++i) {
+        double r = ar[i], im = ai[i];
+        for (int o = 16; o > 0; o >>= 1) {
+            r += __shfl_down_sync(0xffffffffu, r, o);
+            im += __shfl_down_sync(0xffffffffu, im, o);
+        }
+        if (lane == 0) { sr[i][wid] = r; si[i][wid] = im; }
+    }
+    __syncthreads();
+    const unsigned nblocks = gridDim.x * gridDim.y;
+    if (threadIdx.x < KC) {
+        const int i = threadIdx.x;
+        if (i < kc) {
+            double r = 0, im = 0;
+            for (int q = 0; q < RT / 32; ++q) { r += sr[i][q]; im += si[i][q]; }
+            part[(size_t)(c0 + i) * gridDim.x + blockIdx.x] = cmake(r, im);
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == nblocks - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int i = threadIdx.x; i < k; i += blockDim.x) {
+        double r = 0, im = 0;
+        for (unsigned b = 0; b < gridDim.x; ++b) {
+            const cplx p = __ldcg(&part[(size_t)i * gridDim.x + b]);
+            r += p.x; im += p.y;
+        }
+        h[i] = cmake(r, im);
+    }
+    if (threadIdx.x == 0) *counter = 0;
+}
+
+// out = w - sum_i hsub_i V_i and nrm2 = |out|^2 in one launch (last-block
+// reduction as in cgs_pass_kernel).
+__global__ void __launch_bounds__(RT) axpy_norm_kernel(long long n, int k, const cplx* __restrict__ V,
+                                                       const cplx* __restrict__ w, const cplx* __restrict__ hsub,
+                                                       cplx* __restrict__ out, cplx* __restrict__ part,
+                                                       unsigned* __restrict__ counter, cplx* __restrict__ nrm2) {
+    __shared__ cplx hs[MAXM];
+    __shared__ double s[RT];
+    __shared__ bool last;
+    for (int i = threadIdx.x; i < k; i += blockDim.x) hs[i] = hsub[i];
+    __syncthreads();
+    double acc = 0;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+         e += (long long)gridDim.x * blockDim.x) {
+        cplx b = w[e];
+        for (int i = 0; i < k; ++i) b = csub(b, cmul(hs[i], V[(size_t)i * n + e]));
+        out[e] = b;
+        acc += b.x * b.x + b.y * b.y;
+    }
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int st = RT / 2; st > 0; st >>= 1) {
+        if ((int)threadIdx.x < st) s[threadIdx.x] += s[threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = cmake(s[0], 0);
+        __threadfence();
+        last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    acc = 0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) acc += __ldcg(&part[i]).x;
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int st = RT / 2; st > 0; st >>= 1) {
+        if ((int)threadIdx.x < st) s[threadIdx.x] += s[threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        nrm2[0] = cmake(s[0], 0);
+        *counter = 0;
+    }
+}
+
 __global__ void random_kernel(long long n, uint64_t seed, cplx* __restrict__ x) {
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
          e += (long long)gridDim.x * blockDim.x) {
@@ -131,16 +252,6 @@ struct RitzOut {
     double theta, res, beta, tnorm;
 };
 
-// T(i,j) = T(j,i) = Re(h1_i + h2_i), i <= j
-__global__ void fill_t_kernel(int j, const cplx* __restrict__ h1, const cplx* __restrict__ h2,
-                              double* __restrict__ T) {
-    for (int i = threadIdx.x; i <= j; i += blockDim.x) {
-        double v = h1[i].x + h2[i].x;
-        T[i + MAXT * j] = v;
-        T[j + MAXT * i] = v;
-    }
-}
-
 // after a thick restart: T = diag(theta_0 .. theta_{k-1}), zero elsewhere
 __global__ void restart_t_kernel(int k, const double* __restrict__ theta, double* __restrict__ T) {
     for (int e = threadIdx.x; e < MAXT * MAXT; e += blockDim.x) {
@@ -154,14 +265,24 @@ __global__ void restart_t_kernel(int k, const double* __restrict__ theta, double
 // decreasing magnitude) into theta[], vectors into S (m x m complex,
 // column-major); out gets the wanted pair's value and Ritz estimate
 // beta_j |s_{m-1,0}| (beta_j = sqrt(nrm2)).
-__global__ void ritz_kernel(int m, const double* __restrict__ T, const cplx* __restrict__ nrm2, int which,
-                            RitzOut* __restrict__ out, cplx* __restrict__ S, double* __restrict__ theta) {
+__global__ void ritz_kernel(int m, double* __restrict__ T, const cplx* __restrict__ h1, const cplx* __restrict__ h2,
+                            const cplx* __restrict__ nrm2, int which, RitzOut* __restrict__ out,
+                            cplx* __restrict__ S, double* __restrict__ theta) {
     __shared__ double A[MAXT][MAXT + 1], Vv[MAXT][MAXT + 1];
     __shared__ double cs[MAXT / 2], sn[MAXT / 2];
     __shared__ int pa[MAXT / 2], pb[MAXT / 2];
     __shared__ int perm[MAXT];
     const int lane = threadIdx.x;
     const int mp = m + (m & 1);
+    if (h1) {   // new column m-1 of T from the Gram-Schmidt coefficients (T(i,j) = Re(h1_i + h2_i))
+        for (int i = lane; i < m; i += 32) {
+            const double v = h1[i].x + h2[i].x;
+            T[i + MAXT * (m - 1)] = v;
+            T[(m - 1) + MAXT * i] = v;
+        }
+        __syncwarp();
+        __threadfence_block();
+    }
     for (int c = 0; c < mp; ++c) {
         double v = 0.0;
         if (lane < m && c < m) v = 0.5 * (T[lane + MAXT * c] + T[c + MAXT * lane]);
@@ -451,13 +572,26 @@ int optimize_site(Context& ctx, int bl, int br, const MpoSite& op, const cplx* L
     const double eps23 = std::pow(eps, 2.0 / 3.0);
     uint64_t seed = 0x5EEDull + (uint64_t)n * 7919ull;
 
-    auto orthogonalise = [&](cplx* v, int k) {  // CGS2 of v against V_0..V_{k-1}, then P filter
-        multi_dotc(ctx, n, k, V, v, h1);
-        multi_axpy(ctx, n, k, V, h1, -1.0, v);
-        multi_dotc(ctx, n, k, V, v, h2);
-        multi_axpy(ctx, n, k, V, h2, -1.0, v);
-        filt.apply(ctx, n, v);
-        znrm2sq(ctx, n, v, nr);
+    // CGS2 of v against V_0..V_{k-1}, then the P filter: h1 = V^H v,
+    // h2 = V^H (v - V h1), v <- v - V h1 - V h2, nr = |v|^2, in three launches
+    cplx* vtmp = ctx.arena.alloc_n<cplx>(n);
+    const int cgs_nb = (int)std::min<long long>(RB, std::max<long long>(1, (n + RT - 1) / RT));
+    cplx* cgs_part = ctx.arena.alloc_n<cplx>((size_t)cgs_nb * (MAXT / KC + 1) * KC);
+    unsigned* counter = ctx.reduction_counter();
+    auto orthogonalise = [&](cplx* v, int k) {
+        NC_ARG(k <= MAXT + 1, "Krylov basis too large");
+        const dim3 grid(cgs_nb, (k + KC - 1) / KC);
+        cgs_pass_kernel<<<grid, RT, 0, ctx.stream>>>(n, k, V, v, nullptr, nullptr, cgs_part, counter, h1);
+        NC_CHECK_LAUNCH();
+        cgs_pass_kernel<<<grid, RT, 0, ctx.stream>>>(n, k, V, v, h1, vtmp, cgs_part, counter, h2);
+        NC_CHECK_LAUNCH();
+        axpy_norm_kernel<<<cgs_nb, RT, 0, ctx.stream>>>(n, k, V, vtmp, h2, v, cgs_part, counter, nr);
+        NC_CHECK_LAUNCH();
+        ctx.launches += 3;
+        if (filt.r > 0) {
+            filt.apply(ctx, n, v);
+            znrm2sq(ctx, n, v, nr);
+        }
     };
     // starting vector: the projected guess (core.f95:2454), or random if it vanishes
     zcopy(ctx, n, guess, V);
@@ -482,11 +616,9 @@ int optimize_site(Context& ctx, int bl, int br, const MpoSite& op, const cplx* L
         filt.apply(ctx, n, w);
         ++st.matvecs;
         orthogonalise(w, j + 1);
-        fill_t_kernel<<<1, 32, 0, ctx.stream>>>(j, h1, h2, T);
+        ritz_kernel<<<1, 32, 0, ctx.stream>>>(j + 1, T, h1, h2, nr, which, ro, S, theta);
         NC_CHECK_LAUNCH();
-        ritz_kernel<<<1, 32, 0, ctx.stream>>>(j + 1, T, nr, which, ro, S, theta);
-        NC_CHECK_LAUNCH();
-        ctx.launches += 2;
+        ctx.launches++;
         RitzOut rr;
         read_scalars(ctx, ro, sizeof(RitzOut), &rr);
         const double anorm = std::max(std::fabs(rr.theta), eps23);

@@ -101,6 +101,11 @@ struct Context {
     // arena, or a captured graph's private arena while it is being recorded.
     Arena* ws_override = nullptr;
     Arena& scratch() { return ws_override ? *ws_override : arena; }
+    // Completion counter of single-kernel reductions (the last block to finish
+    // combines the partial sums in a fixed order and resets it to zero); one
+    // per context, used in stream order only.
+    unsigned* red_counter = nullptr;
+    unsigned* reduction_counter();
     // Kernel timing (nc_profile_begin/end): CUDA events around every complex
     // GEMM of at least profile_min_flops, on the launching stream.
     bool profile = false;

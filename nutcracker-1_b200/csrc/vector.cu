@@ -87,7 +87,16 @@ Context::Context() {
     NC_CUDA(cudaMallocHost(&pinned, pinned_bytes));
 }
 
+unsigned* Context::reduction_counter() {
+    if (!red_counter) {
+        NC_CUDA(cudaMalloc(&red_counter, 64 * sizeof(unsigned)));
+        NC_CUDA(cudaMemset(red_counter, 0, 64 * sizeof(unsigned)));
+    }
+    return red_counter;
+}
+
 Context::~Context() {
+    if (red_counter) cudaFree(red_counter);
     if (own_stream) cudaStreamDestroy(own_stream);
     if (pinned) cudaFreeHost(pinned);
 }
@@ -126,10 +135,14 @@ __global__ void permute3_kernel(const cplx* __restrict__ in, int o0, int o1, int
     }
 }
 
+// <x,y> (or |x|^2) in one launch: every block stores its partial sum, and the
+// last block to finish (by an atomic ticket after a fence) adds the partials
+// in block order, so the result does not depend on block timing.
 template <bool NORM>
-__global__ void dot_partial(long long n, const cplx* __restrict__ x, const cplx* __restrict__ y,
-                            cplx* __restrict__ part) {
+__global__ void dot_fused(long long n, const cplx* __restrict__ x, const cplx* __restrict__ y,
+                          cplx* __restrict__ part, unsigned* __restrict__ counter, cplx* __restrict__ out) {
     __shared__ double sr[RED_THREADS], si[RED_THREADS];
+    __shared__ bool last;
     double ar = 0, ai = 0;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
          e += (long long)gridDim.x * blockDim.x) {
@@ -148,20 +161,29 @@ __global__ void dot_partial(long long n, const cplx* __restrict__ x, const cplx*
         if ((int)threadIdx.x < s) { sr[threadIdx.x] += sr[threadIdx.x + s]; si[threadIdx.x] += si[threadIdx.x + s]; }
         __syncthreads();
     }
-    if (threadIdx.x == 0) part[blockIdx.x] = cmake(sr[0], si[0]);
-}
-
-__global__ void reduce_final(int n, const cplx* __restrict__ part, cplx* __restrict__ out) {
-    __shared__ double sr[RED_THREADS], si[RED_THREADS];
-    double ar = 0, ai = 0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) { ar += part[i].x; ai += part[i].y; }
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = cmake(sr[0], si[0]);
+        __threadfence();
+        last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    ar = 0; ai = 0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
+        const cplx p = __ldcg(&part[i]);
+        ar += p.x; ai += p.y;
+    }
     sr[threadIdx.x] = ar; si[threadIdx.x] = ai;
     __syncthreads();
     for (int s = RED_THREADS / 2; s > 0; s >>= 1) {
         if ((int)threadIdx.x < s) { sr[threadIdx.x] += sr[threadIdx.x + s]; si[threadIdx.x] += si[threadIdx.x + s]; }
         __syncthreads();
     }
-    if (threadIdx.x == 0) out[0] = cmake(sr[0], si[0]);
+    if (threadIdx.x == 0) {
+        out[0] = cmake(sr[0], si[0]);
+        *counter = 0;
+    }
 }
 
 __global__ void copy_kernel(long long n, const cplx* __restrict__ x, cplx* __restrict__ y) {
@@ -211,21 +233,19 @@ void permute3(Context& ctx, const cplx* in, int n0, int n1, int n2, const int pe
 void zdotc(Context& ctx, long long n, const cplx* x, const cplx* y, cplx* result) {
     ArenaFrame f(ctx.arena);
     cplx* part = ctx.arena.alloc_n<cplx>(RED_BLOCKS);
-    dot_partial<false><<<RED_BLOCKS, RED_THREADS, 0, ctx.stream>>>(n, x, y, part);
+    const unsigned nb = (unsigned)std::max<long long>(1, std::min<long long>(RED_BLOCKS, (n + RED_THREADS - 1) / RED_THREADS));
+    dot_fused<false><<<nb, RED_THREADS, 0, ctx.stream>>>(n, x, y, part, ctx.reduction_counter(), result);
     NC_CHECK_LAUNCH();
-    reduce_final<<<1, RED_THREADS, 0, ctx.stream>>>(RED_BLOCKS, part, result);
-    NC_CHECK_LAUNCH();
-    ctx.launches += 2;
+    ctx.launches++;
 }
 
 void znrm2sq(Context& ctx, long long n, const cplx* x, cplx* result) {
     ArenaFrame f(ctx.arena);
     cplx* part = ctx.arena.alloc_n<cplx>(RED_BLOCKS);
-    dot_partial<true><<<RED_BLOCKS, RED_THREADS, 0, ctx.stream>>>(n, x, x, part);
+    const unsigned nb = (unsigned)std::max<long long>(1, std::min<long long>(RED_BLOCKS, (n + RED_THREADS - 1) / RED_THREADS));
+    dot_fused<true><<<nb, RED_THREADS, 0, ctx.stream>>>(n, x, x, part, ctx.reduction_counter(), result);
     NC_CHECK_LAUNCH();
-    reduce_final<<<1, RED_THREADS, 0, ctx.stream>>>(RED_BLOCKS, part, result);
-    NC_CHECK_LAUNCH();
-    ctx.launches += 2;
+    ctx.launches++;
 }
 
 void zcopy(Context& ctx, long long n, const cplx* x, cplx* y) {
