@@ -73,6 +73,31 @@ struct DevBuf {
     void release() { if (p) cudaFreeAsync(p, s); p = nullptr; n = 0; }
 };
 
+// Second stream (and its two events) on which a move's neighbour absorbs the
+// gauge factor while the environment update runs on the chain's stream.
+struct SideStream {
+    AbsorbAsync a{nullptr, nullptr, nullptr};
+    SideStream() {
+        cudaError_t e = cudaStreamCreateWithFlags(&a.stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&a.ready, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&a.done, cudaEventDisableTiming);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            destroy();
+            throw Error(NC_ERR_CUDA, std::string("chain: side stream: ") + cudaGetErrorString(e));
+        }
+    }
+    SideStream(const SideStream&) = delete;
+    SideStream& operator=(const SideStream&) = delete;
+    ~SideStream() { destroy(); }
+    void destroy() {
+        if (a.stream) { cudaStreamSynchronize(a.stream); cudaStreamDestroy(a.stream); }
+        if (a.ready) cudaEventDestroy(a.ready);
+        if (a.done) cudaEventDestroy(a.done);
+        a = AbsorbAsync{nullptr, nullptr, nullptr};
+    }
+};
+
 struct OpSite {
     MpoSite dev;
     DevBuf W;
@@ -125,6 +150,7 @@ struct Chain {
     std::vector<std::vector<DevBuf>> Lov, Rov;   // [projector][site]
     std::vector<std::vector<ProjSite>> projectors;
     DevBuf spare_a, spare_b;
+    SideStream side;
     // projector matrix of the current site
     DevBuf pm_refl, pm_tau;
     DevProjector pm;
@@ -386,14 +412,20 @@ struct Chain {
                 // site c -> left-normalised, site c+1 absorbs the factor and becomes the centre
                 PhaseTimer t(opt.time_phases, ctx.stream, &stats.t_gauge);
                 gauge_right(ctx, bl(c), br(c), br(c + 1), phys[c], phys[c + 1], site[c].p, site[c + 1].p,
-                            spare_a.p, spare_b.p);
+                            spare_a.p, spare_b.p, &side.a);
                 std::swap(site[c], spare_a);
                 std::swap(site[c + 1], spare_b);
-                normalize(site[c + 1].p, (long long)site_elems(c + 1));
             }
             {
+                // the environment update needs only the normalised site c, so it
+                // overlaps the absorption GEMM running on the side stream
                 PhaseTimer t(opt.time_phases, ctx.stream, &stats.t_env);
                 absorb_left(c);
+            }
+            {
+                PhaseTimer t(opt.time_phases, ctx.stream, &stats.t_gauge);
+                NC_CUDA(cudaStreamWaitEvent(ctx.stream, side.a.done, 0));
+                normalize(site[c + 1].p, (long long)site_elems(c + 1));
             }
             cur = c + 1;
         } else {
@@ -401,14 +433,18 @@ struct Chain {
             {
                 PhaseTimer t(opt.time_phases, ctx.stream, &stats.t_gauge);
                 gauge_left(ctx, bl(c - 1), br(c - 1), br(c), phys[c - 1], phys[c], site[c - 1].p, site[c].p,
-                           spare_a.p, spare_b.p);
+                           spare_a.p, spare_b.p, &side.a);
                 std::swap(site[c - 1], spare_a);
                 std::swap(site[c], spare_b);
-                normalize(site[c - 1].p, (long long)site_elems(c - 1));
             }
             {
                 PhaseTimer t(opt.time_phases, ctx.stream, &stats.t_env);
                 absorb_right(c);
+            }
+            {
+                PhaseTimer t(opt.time_phases, ctx.stream, &stats.t_gauge);
+                NC_CUDA(cudaStreamWaitEvent(ctx.stream, side.a.done, 0));
+                normalize(site[c - 1].p, (long long)site_elems(c - 1));
             }
             cur = c - 1;
         }

@@ -198,12 +198,20 @@ void sos_right_mixed(Context& ctx, int bl, int br, const MpoSite& op, const cplx
 // C (M x N) = A (M x K) B (K x N), column-major complex128, through tc_gemm;
 // three = false uses one TF32 product.  Synchronises and checks tc_check.
 void tc_zgemm(Context& ctx, int M, int N, int K, const cplx* A, const cplx* B, cplx* C, bool three);
-// A (bm,bl,dl) -> normA left-normalised; B (br,bm,dr) absorbs the factor.
+// Second stream for the neighbour's absorption of the gauge factor: the GEMM
+// waits on `ready` (recorded on ctx.stream after the QR), runs on `stream` and
+// records `done`, which the caller waits on before it reads the absorbed site.
+struct AbsorbAsync {
+    cudaStream_t stream;
+    cudaEvent_t ready, done;
+};
+// A (bm,bl,dl) -> normA left-normalised; B (br,bm,dr) absorbs the factor
+// (on async->stream when async is given).
 void gauge_right(Context& ctx, int bl, int bm, int br, int dl, int dr, const cplx* A, const cplx* B,
-                 cplx* normA, cplx* denormB);
+                 cplx* normA, cplx* denormB, const AbsorbAsync* async = nullptr);
 // B (br,bm,dr) -> normB right-normalised; A (bm,bl,dl) absorbs the factor.
 void gauge_left(Context& ctx, int bl, int bm, int br, int dl, int dr, const cplx* A, const cplx* B,
-                cplx* denormA, cplx* normB);
+                cplx* denormA, cplx* normB, const AbsorbAsync* async = nullptr);
 void rand_norm_site(Context& ctx, int br, int bl, int d, uint64_t seed, cplx* out);
 void rand_unnorm_site(Context& ctx, int br, int bl, int d, uint64_t seed, cplx* out);
 void increase_bandwidth(Context& ctx, int bl, int bm, int br, int dl, int dr, int new_bm, uint64_t seed,

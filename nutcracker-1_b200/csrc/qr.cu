@@ -848,26 +848,40 @@ void qr_run(Context& ctx, QrPlan& P) {
 }
 }  // namespace
 
+// The absorption GEMM of the gauge factor, on ctx.stream or, with `as`, on
+// the second stream after the QR that produced the factor.
+static void absorb_factor(Context& ctx, const ZGemmParams& p, const AbsorbAsync* as) {
+    if (!as) {
+        zgemm(p, ctx);
+        return;
+    }
+    NC_CUDA(cudaEventRecord(as->ready, ctx.stream));
+    NC_CUDA(cudaStreamWaitEvent(as->stream, as->ready, 0));
+    zgemm(p, as->stream);
+    ctx.launches++;
+    NC_CUDA(cudaEventRecord(as->done, as->stream));
+}
+
 void gauge_right(Context& ctx, int bl, int bm, int br, int dl, int dr, const cplx* A, const cplx* B,
-                 cplx* normA, cplx* denormB) {
+                 cplx* normA, cplx* denormB, const AbsorbAsync* async) {
     const int K = bl * dl;
     NC_ARG(K >= bm, "not enough degrees of freedom to normalize");
     QrPlan& P = qr_plan(ctx, K, bm, false);
     const int p_t[3] = {1, 0, 2};
     permute3(ctx, A, bm, K, 1, p_t, true, P.X);             // X = A^H  (K x bm)
     qr_run(ctx, P);                                          // A^H = Qt Rt
-    permute3(ctx, P.Q, K, bm, 1, p_t, true, normA);         // normA = Qt^H
     if (B && denormB) {
         // denormB_s = B_s Rt^H  (neighbour absorbs P = Rt^H on its left index)
         ZGemmParams p = zgemm_params(OP_N, OP_C, br, bm, bm, B, br, P.R, bm, denormB, br);
         p.batch = dr;
         p.sA0 = (long long)br * bm; p.sB0 = 0; p.sC0 = (long long)br * bm;
-        zgemm(p, ctx);
+        absorb_factor(ctx, p, async);
     }
+    permute3(ctx, P.Q, K, bm, 1, p_t, true, normA);         // normA = Qt^H
 }
 
 void gauge_left(Context& ctx, int bl, int bm, int br, int dl, int dr, const cplx* A, const cplx* B,
-                cplx* denormA, cplx* normB) {
+                cplx* denormA, cplx* normB, const AbsorbAsync* async) {
     const int K = br * dr;
     NC_ARG(K >= bm, "not enough degrees of freedom to normalize");
     QrPlan& P = qr_plan(ctx, K, bm, true);
@@ -875,11 +889,11 @@ void gauge_left(Context& ctx, int bl, int bm, int br, int dl, int dr, const cplx
     const int p_rs[3] = {0, 2, 1};
     permute3(ctx, B, br, bm, dr, p_rs, true, P.X);           // X((r,s),m) = conj(B(r,m,s))
     qr_run(ctx, P);                                          // Rc = conj(Rt)
-    permute3(ctx, P.Q, br, dr, bm, p_rs, true, normB);       // normB(r,m,s) = conj(Qt((r,s),m))
     if (A && denormA) {
         // denormA = conj(Rt) * A  (as bm x bl*dl)
-        zgemm(zgemm_params(OP_N, OP_N, bm, bl * dl, bm, Rc, bm, A, bm, denormA, bm), ctx);
+        absorb_factor(ctx, zgemm_params(OP_N, OP_N, bm, bl * dl, bm, Rc, bm, A, bm, denormA, bm), async);
     }
+    permute3(ctx, P.Q, br, dr, bm, p_rs, true, normB);       // normB(r,m,s) = conj(Qt((r,s),m))
 }
 
 void rand_norm_site(Context& ctx, int br, int bl, int d, uint64_t seed, cplx* out) {
