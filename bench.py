@@ -53,6 +53,9 @@ UNIT = "sweeps/s"
 # with ncv=3, which the reference uses, needs several times more, so the CPU
 # figure is an upper bound on the reference's speed).
 CPU_SAMPLE_MATVECS = 1.37
+# DRAM traffic of one tcgen05 stage-A GEMM launch at chi=1024 (ncu, read 216.9 MB +
+# write 48.0 MB; the shape's algorithmic operand bytes are 185 MB).
+TC32_PROFILED_TRAFFIC = 264.9e6
 
 
 def parse():
@@ -81,6 +84,12 @@ def parse():
                     help="requests of the same stream timed one at a time (the plain per-solve baseline)")
     ap.add_argument("--serve-slots", type=int, default=0, help="concurrent requests (0: min(16, cores - 2))")
     ap.add_argument("--serve-rate", type=float, default=64.0, help="Poisson arrival rate, requests/s")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-form sample")
+    ap.add_argument("--batched-only", action="store_true", help="run only the batched-form sample")
+    ap.add_argument("--batch-chains", type=int, default=32,
+                    help="chains in the batched sample (the batched workload has 4096; a bounded sample)")
+    ap.add_argument("--batch-plain", type=int, default=6,
+                    help="chains of the same batch solved one at a time (the plain per-chain baseline)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--phases", action="store_true",
                     help="synchronise and time each sweep phase (diagnostics; slows the sweep slightly)")
@@ -175,6 +184,24 @@ def run_tc_gemm_only(args):
                       "tf32_tflops": fl.value / (ms.value * 1e-3) / 1e12 if ms.value > 0 else None}), flush=True)
 
 
+def tfim_exact_levels(n, lam, k):
+    """Lowest k levels of the open chain H = -sum Z_i Z_{i+1} - lam sum X_i, exact
+    at any N from its free-fermion form (Jordan-Wigner; Lieb, Schultz & Mattis 1961):
+    with A = 2 lam I minus the nearest-neighbour ones and the antisymmetric pairing B
+    (B[i,i+1] = -1), the BdG matrix [[A, B], [-B, -A]] has eigenvalues +-L_k, and the
+    spectrum is -sum(L)/2 plus the sum of any subset of the L_k."""
+    A = np.diag(np.full(n, 2.0 * lam))
+    B = np.zeros((n, n))
+    for i in range(n - 1):
+        A[i, i + 1] = A[i + 1, i] = -1.0
+        B[i, i + 1], B[i + 1, i] = -1.0, 1.0
+    L = np.sort(np.abs(np.linalg.eigvalsh(np.block([[A, B], [-B, -A]]))[n:]))
+    e0 = -0.5 * float(L.sum())
+    m = min(n, 4)
+    levels = sorted(e0 + sum(float(L[i]) for i in range(m) if mask >> i & 1) for mask in range(1 << m))
+    return levels[:k]
+
+
 def serving_sample(args):
     """Serving workload sample: transverse-field Ising solves H = -sum ZZ - lam sum X with
     lam ~ U[0.5,1.5], N ~ U{8..128}, chi ~ U{16..256} (capped at the chain's maximum bond
@@ -183,7 +210,6 @@ def serving_sample(args):
     submits the whole stream on its arrival schedule to a server with several slots."""
     from nutcracker_b200 import operators
     from nutcracker_b200.serve import Server
-    from oracle import ed, mpo
 
     rng = np.random.default_rng(args.seed + 5)
     reqs = []
@@ -237,12 +263,14 @@ def serving_sample(args):
     failed = [i for i, x in enumerate(res) if x["status"] != 0]
     same = max((abs(a - b) / max(abs(a), 1e-300) for p, m in zip(plain, res) for a, b in
                 zip(p["energies"], m["energies"])), default=0.0)
-    ed_err = []
+    exact_err, exact_err_full_chi = [], []
     for r, x in zip(reqs, res):
         n, lam, chi, levels = r
-        if n <= 12 and x["status"] == 0:
-            w, _ = ed.lowest_levels(mpo.transverse_ising_ferro(n, lam), levels)
-            ed_err.append(max(abs(e - ref) / n for e, ref in zip(x["energies"], w)))
+        if x["status"] == 0:
+            err = max(abs(e - ref) / n for e, ref in zip(x["energies"], tfim_exact_levels(n, lam, levels)))
+            exact_err.append(err)
+            if chi >= 2 ** (n // 2):   # the bond dimension represents the chain exactly
+                exact_err_full_chi.append(err)
     plain_rate = len(plain) / t_plain if t_plain > 0 else None
     return {
         "workload": "TFIM -ZZ - lam X: lam~U[0.5,1.5], N~U{8..%d}, chi~U{16..%d} (<= chain maximum), "
@@ -256,28 +284,111 @@ def serving_sample(args):
         "plain_solves_per_s": plain_rate, "plain_requests": len(plain),
         "speedup_vs_plain": (st["solves_per_second"] / plain_rate) if plain_rate else None,
         "max_rel_diff_alone_vs_mix": same,
-        "ed_checked": len(ed_err), "max_dE_per_site_vs_ed": max(ed_err) if ed_err else None,
+        "max_dE_per_site_vs_exact": max(exact_err) if exact_err else None,
+        "max_dE_per_site_vs_exact_where_chi_is_exact": max(exact_err_full_chi) if exact_err_full_chi else None,
+        "exact": "free-fermion levels of every request (truncation error included where chi < 2^(N/2))",
+    }
+
+
+def batched_sample(args):
+    """Batched workload sample: independent XXZ chains H = sum_i J_i (XX + YY + Delta_i ZZ)
+    with per-bond J_i ~ U[0.5,1.5], Delta_i ~ U[0,2], N ~ U{8..48}, chi ~ U{8..128} (capped
+    at the chain's maximum bond dimension), ground state in FP64, seeded.  The first
+    `batch_plain` chains are solved one at a time (the plain per-chain throughput); the
+    batch is then submitted at once to the serving engine, whose workers (each with its
+    own stream and arena) keep many chains in flight on the GPU."""
+    from nutcracker_b200 import operators
+    from nutcracker_b200.serve import Server
+
+    rng = np.random.default_rng(args.seed + 11)
+    chains = []
+    for _ in range(args.batch_chains):
+        n = int(rng.integers(8, 49))
+        chi = int(min(rng.integers(8, 129), 2 ** (n // 2)))
+        chains.append((n, operators.xxz_random(n, rng), chi))
+    slots = args.serve_slots or max(1, min(16, os.cpu_count() or 4))
+
+    def submit(srv, k):
+        n, op, chi = chains[k]
+        return srv.submit(op, levels=1, initial_bandwidth_dimension=chi, seed=3000 + k)
+
+    with Server(max_inflight=slots) as srv:
+        warm = operators.xxz_random(16, np.random.default_rng(1))
+        for i in [srv.submit(warm, levels=1, initial_bandwidth_dimension=16, seed=1) for _ in range(slots)]:
+            srv.wait(i)
+        plain = []
+        t0 = time.perf_counter()
+        for k in range(min(args.batch_plain, len(chains))):
+            plain.append(srv.wait(submit(srv, k)))
+        t_plain = time.perf_counter() - t0
+        start = time.perf_counter()
+        ids = [submit(srv, k) for k in range(len(chains))]
+        res = [srv.wait(i) for i in ids]
+        window = time.perf_counter() - start
+    ok = [x for x in res if x["status"] == 0]
+    same = max((abs(p["energies"][0] - m["energies"][0]) / max(abs(p["energies"][0]), 1e-300)
+                for p, m in zip(plain, res)), default=0.0)
+    plain_rate = len(plain) / t_plain if t_plain > 0 else None
+    rate = len(ok) / window if window > 0 else None
+    return {
+        "workload": "XXZ chains sum J_i (XX + YY + Delta_i ZZ): J_i~U[0.5,1.5], Delta_i~U[0,2] per bond, "
+                    "N~U{8..48}, chi~U{8..128} (<= chain maximum), ground state, FP64; %d chains (bounded "
+                    "sample of the 4096-chain batch)" % len(chains),
+        "slots": slots, "chains": len(chains), "failed": len(chains) - len(ok),
+        "chains_per_s": rate, "window_s": window,
+        "plain_chains_per_s": plain_rate, "plain_chains": len(plain),
+        "speedup_vs_plain": (rate / plain_rate) if (rate and plain_rate) else None,
+        "max_rel_diff_alone_vs_batch": same,
     }
 
 
 def run_gauge_only(args):
     """W + K right-moving gauge moves (norm_denorm_going_right_) of a
-    (chi, chi, 2) site into its neighbour, through the Level-0 C-ABI."""
+    (chi, chi, 2) site into its neighbour: device-resident through
+    nc_gauge_move_dev, timed with CUDA events on the library's stream, and
+    once through the Level-0 host entry point (host copies included)."""
+    import ctypes as ct
     import time as _t
+
+    import torch
 
     import nutcracker_b200 as nb
 
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    nb.lib.nc_set_stream(ct.c_void_p(stream.cuda_stream))
     rng = np.random.default_rng(args.seed)
     chi = args.chi
     A = np.asfortranarray(rng.standard_normal((chi, chi, 2)) + 1j * rng.standard_normal((chi, chi, 2)))
     B = np.asfortranarray(rng.standard_normal((chi, chi, 2)) + 1j * rng.standard_normal((chi, chi, 2)))
-    for _ in range(args.warmup):
-        nb.Core.norm_denorm_going_right(chi, chi, chi, 2, 2, A, B)
-    t0 = _t.perf_counter()
+    dA = torch.from_numpy(A.ravel(order="F")).cuda()
+    dB = torch.from_numpy(B.ravel(order="F")).cuda()
+    oA, oB = torch.empty_like(dA), torch.empty_like(dB)
+    args_dev = [ct.c_void_p(t.data_ptr()) for t in (dA, dB, oA, oB)]
+
+    def once():
+        if nb.lib.nc_gauge_move_dev(1, chi, chi, chi, 2, 2, *args_dev) != 0:
+            nb._check()
+
+    for _ in range(max(1, args.warmup)):
+        once()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("timed")
+    e0.record(stream)
     for _ in range(args.steps):
-        nb.Core.norm_denorm_going_right(chi, chi, chi, 2, 2, A, B)
-    t = (_t.perf_counter() - t0) / args.steps
-    print(json.dumps({"gauge_chi": chi, "ms_with_host_copies": t * 1e3}), flush=True)
+        once()
+    e1.record(stream)
+    torch.cuda.nvtx.range_pop()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    t0 = _t.perf_counter()
+    nb.Core.norm_denorm_going_right(chi, chi, chi, 2, 2, A, B)
+    t_host = _t.perf_counter() - t0
+    m, n = 2 * chi, chi
+    flops = 4.0 * (2 * m * n * n - 2.0 / 3.0 * n ** 3)
+    print(json.dumps({"gauge_chi": chi, "ms": ms, "qr_equiv_tflops": flops / (ms * 1e-3) / 1e12,
+                      "ms_with_host_copies": t_host * 1e3}), flush=True)
 
 
 # ---------------------------------------------------------------------------
@@ -625,7 +736,11 @@ def run_ours(args, rank, world):
                      "gpu_launches": int(r["launches"])})
         line["roofline"] = {"bound": "tensor", "kernel": "tc32_gemm_kernel (tcgen05 kind::tf32, 3xTF32 complex GEMM)",
                             "achieved": ach, "peak": peak_tf32, "unit": "TFLOP/s",
-                            "frac": ach / peak_tf32 if ach else None, "traffic": None,
+                            "frac": ach / peak_tf32 if ach else None,
+                            "traffic": TC32_PROFILED_TRAFFIC, "traffic_unit": "bytes per launch",
+                            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one stage-A "
+                                              "launch (M=1024, N=5120, K=1024), profiles/tc32_gemm_3xtf32.md; "
+                                              "algorithmic operand bytes of that launch 185 MB",
                             "flops_counted": "TF32 tensor work: 2*M*Nr*Kr per segment, 3 segments",
                             "peak_source": peak_src, "timed_gemms": r["tc"][0],
                             "gemm_share_of_step": ms / r["seconds"],
@@ -646,6 +761,8 @@ def run_ours(args, rank, world):
                      "roofline": line["fp64"]["roofline"], "chain": line["fp64"]["chain"]})
     if world == 1 and not args.no_serving:
         line["serving"] = serving_sample(args)
+    if world == 1 and not args.no_batched:
+        line["batched"] = batched_sample(args)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.sites, args.chi)
     print(json.dumps(line), flush=True)
@@ -667,6 +784,8 @@ def main():
             run_heff_only(args)
         elif args.tc_gemm_only:
             run_tc_gemm_only(args)
+        elif args.batched_only:
+            print(json.dumps({"batched": batched_sample(args)}), flush=True)
         elif args.serving_only:
             import torch
             torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))

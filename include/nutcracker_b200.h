@@ -85,6 +85,15 @@ int nc_env_update_dev(int side, int mixed, uint32_t bl, uint32_t br, uint32_t cl
                       uint32_t nnz, const uint32_t* idx_dev, const void* W_dev, const void* env_dev,
                       const void* psi_dev, void* out_dev);
 
+/* Device-pointer gauge move (norm_denorm_going_right_ / _left_ of
+   core.f95:2708-2878, QR gauge): direction > 0 left-normalises A (bm,bl,dl)
+   into out_A and lets B (br,bm,dr) absorb the factor into out_B; direction < 0
+   right-normalises B into out_B and lets A absorb the factor into out_A.  All
+   buffers in device memory; inputs are not modified.  Asynchronous on this
+   thread's stream; returns a status code. */
+int nc_gauge_move_dev(int direction, uint32_t bl, uint32_t bm, uint32_t br, uint32_t dl, uint32_t dr,
+                      const void* A_dev, const void* B_dev, void* out_A_dev, void* out_B_dev);
+
 /* C = A B for column-major complex128 device matrices A (M x K), B (K x N),
    C (M x N) on the tcgen05 tensor cores: 3xTF32 when `three` is nonzero,
    else one TF32 product.  The GEMM under the precision form, exposed for

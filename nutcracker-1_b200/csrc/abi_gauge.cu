@@ -51,6 +51,21 @@ int32_t norm_denorm_going_right_(const uint32_t* bl, const uint32_t* bm, const u
     return g_status;
 }
 
+int nc_gauge_move_dev(int direction, uint32_t bl, uint32_t bm, uint32_t br, uint32_t dl, uint32_t dr,
+                      const void* A_dev, const void* B_dev, void* out_A_dev, void* out_B_dev) {
+    NC_ABI_BEGIN
+    NC_ARG(direction != 0 && A_dev && B_dev && out_A_dev && out_B_dev, "nc_gauge_move_dev: bad arguments");
+    Context& ctx = Context::get();
+    if (direction > 0)
+        gauge_right(ctx, bl, bm, br, dl, dr, (const cplx*)A_dev, (const cplx*)B_dev, (cplx*)out_A_dev,
+                    (cplx*)out_B_dev);
+    else
+        gauge_left(ctx, bl, bm, br, dl, dr, (const cplx*)A_dev, (const cplx*)B_dev, (cplx*)out_A_dev,
+                   (cplx*)out_B_dev);
+    NC_ABI_END
+    return g_status;
+}
+
 int32_t norm_for_left_(const uint32_t* br, const uint32_t* bl, const uint32_t* d, const nc_complex* S,
                        nc_complex* out) {
     NC_ABI_BEGIN

@@ -783,12 +783,32 @@ QrPlan& qr_plan(Context& ctx, int m, int n, bool conjR) {
     p->R = p->arena.alloc_n<cplx>((size_t)n * n);
     if (cluster_qr_available()) {
         p->lookahead = true;
-        p->ev.resize(2 + 2 * ((n + NB - 1) / NB));
+        p->ev.resize(4 + 2 * ((n + NB - 1) / NB));   // the last two fork/join the priority stream
         for (cudaEvent_t& e : p->ev) NC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
     p->capture = n > NB;
     plans.push_back(std::move(p));
     return *plans.back();
+}
+
+// Highest-priority stream of this host thread for the critical path of the
+// recorded look-ahead QR (panels, T, next-block updates).  Graph nodes keep
+// the priority of the stream they were captured from (the graph is
+// instantiated with cudaGraphInstantiateFlagUseNodePriority), so a pending
+// cluster launch is dispatched ahead of the trailing-update GEMMs of the
+// second stream as SMs drain.  Null when the stream cannot be created.
+cudaStream_t priority_stream() {
+    thread_local cudaStream_t s = [] {
+        int least = 0, greatest = 0;
+        cudaStream_t st = nullptr;
+        if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess ||
+            cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, greatest) != cudaSuccess) {
+            cudaGetLastError();
+            st = nullptr;
+        }
+        return st;
+    }();
+    return s;
 }
 
 // Run the QR of plan.X; the first run of a shape executes directly (so the
@@ -825,19 +845,32 @@ void qr_run(Context& ctx, QrPlan& P) {
     try {
         once();
         const uint64_t l0 = ctx.launches;
-        NC_CUDA(cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeRelaxed));
+        const cudaStream_t home = ctx.stream;
+        const cudaStream_t hp = P.lookahead ? priority_stream() : nullptr;
+        NC_CUDA(cudaStreamBeginCapture(home, cudaStreamCaptureModeRelaxed));
         try {
+            if (hp) {
+                NC_CUDA(cudaEventRecord(P.ev[P.ev.size() - 2], home));
+                NC_CUDA(cudaStreamWaitEvent(hp, P.ev[P.ev.size() - 2], 0));
+                ctx.stream = hp;
+            }
             once();
+            if (hp) {
+                NC_CUDA(cudaEventRecord(P.ev[P.ev.size() - 1], hp));
+                ctx.stream = home;
+                NC_CUDA(cudaStreamWaitEvent(home, P.ev[P.ev.size() - 1], 0));
+            }
         } catch (...) {
+            ctx.stream = home;
             cudaGraph_t g = nullptr;
-            cudaStreamEndCapture(ctx.stream, &g);
+            cudaStreamEndCapture(home, &g);
             if (g) cudaGraphDestroy(g);
             throw;
         }
-        NC_CUDA(cudaStreamEndCapture(ctx.stream, &P.graph));
+        NC_CUDA(cudaStreamEndCapture(home, &P.graph));
         P.kernels = ctx.launches - l0;
         ctx.launches = l0;
-        NC_CUDA(cudaGraphInstantiate(&P.exec, P.graph, 0));
+        NC_CUDA(cudaGraphInstantiateWithFlags(&P.exec, P.graph, cudaGraphInstantiateFlagUseNodePriority));
     } catch (...) {
         ctx.ws_override = nullptr;
         ctx.profile = prof;

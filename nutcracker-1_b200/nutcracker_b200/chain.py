@@ -78,6 +78,7 @@ lib.nc_chain_increase_bandwidth_dimension.argtypes = [ct.c_void_p, ct.c_uint32]
 lib.nc_chain_move_to.argtypes = [ct.c_void_p, ct.c_uint32]
 lib.nc_chain_set_precision.argtypes = [ct.c_void_p, ct.c_uint32]
 lib.nc_chain_solve_for_eigenvalues.argtypes = [ct.c_void_p, ct.c_uint32, ct.POINTER(ct.c_double)]
+lib.nc_chain_solve_levels_at_bandwidth.argtypes = [ct.c_void_p, ct.c_uint32, ct.POINTER(ct.c_double)]
 lib.nc_chain_get_energy.argtypes = [ct.c_void_p, ct.POINTER(ct.c_double)]
 lib.nc_chain_compute_expectation_value.argtypes = [ct.c_void_p, ct.POINTER(ct.c_double)]
 lib.nc_chain_get_info.argtypes = [ct.c_void_p, ct.POINTER(nc_chain_info)]
@@ -184,6 +185,12 @@ class Chain:
     def solve_for_eigenvalues(self, n):
         out = (ct.c_double * n)()
         self._call(lib.nc_chain_solve_for_eigenvalues, ct.c_uint32(int(n)), out)
+        return list(out)
+
+    def solve_levels_at_bandwidth(self, n):
+        """n levels at the current bond dimension (nc_chain_solve_levels_at_bandwidth)."""
+        out = (ct.c_double * n)()
+        self._call(lib.nc_chain_solve_levels_at_bandwidth, ct.c_uint32(int(n)), out)
         return list(out)
 
     def get_energy(self):

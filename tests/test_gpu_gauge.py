@@ -128,3 +128,32 @@ def test_form_norm_overlap_tensors(nb):
     # the left-normalised overlap site and the denormalised site 2 carry the same pair
     back = lambda O: np.conj(np.transpose(O, (2, 0, 1)))  # overlap (bl,d,br) -> state (br,bl,d)
     assert rel_err(pair(back(lno), dS2), pair(back(rl), rd)) < 1e-12
+
+
+@pytest.mark.parametrize("direction", [1, -1])
+def test_gauge_move_dev_matches_host_entry(nb, direction):
+    """nc_gauge_move_dev (device pointers) gives the host entry points' results
+    bit for bit, and leaves its inputs unchanged."""
+    import ctypes as ct
+
+    import torch
+
+    bl, bm, br, dl, dr = 256, 300, 256, 2, 2
+    rng = np.random.default_rng(5 + direction)
+    A = rand_c(rng, (bm, bl, dl)); B = rand_c(rng, (br, bm, dr))
+    if direction > 0:
+        _, wantA, wantB = nb.Core.norm_denorm_going_right(bl, bm, br, dl, dr, A, B)
+    else:
+        _, wantA, wantB = nb.Core.norm_denorm_going_left(bl, bm, br, dl, dr, A, B)
+    dA = torch.from_numpy(A.ravel(order="F").copy()).cuda()
+    dB = torch.from_numpy(B.ravel(order="F").copy()).cuda()
+    oA, oB = torch.empty_like(dA), torch.empty_like(dB)
+    torch.cuda.synchronize()
+    st = nb.lib.nc_gauge_move_dev(direction, bl, bm, br, dl, dr, *[ct.c_void_p(t.data_ptr()) for t in (dA, dB, oA, oB)])
+    assert st == 0, nb.lib.nc_last_error()
+    assert nb.lib.nc_synchronize() == 0
+    gotA = oA.cpu().numpy().reshape(A.shape, order="F")
+    gotB = oB.cpu().numpy().reshape(B.shape, order="F")
+    assert np.array_equal(gotA, wantA) and np.array_equal(gotB, wantB)
+    assert np.array_equal(dA.cpu().numpy(), A.ravel(order="F"))
+    assert np.array_equal(dB.cpu().numpy(), B.ravel(order="F"))
