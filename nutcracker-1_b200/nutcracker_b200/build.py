@@ -7,8 +7,11 @@ package requires the library this script produces).
 
 Compiles every ``csrc/*.cu`` with
 ``nvcc -gencode arch=compute_100a,code=sm_100a -O3 -lineinfo`` and links
-``lib/libnutcracker_b200.so``.  Objects go to ``_build/``.  Rebuilds only
-what changed (by mtime against the sources and headers).
+``lib/libnutcracker_b200.so``, then the command-line program
+``programs/nutcracker.cpp`` into ``bin/nutcracker_b200`` (host C++ against the
+library, found through an $ORIGIN-relative rpath).  Objects go to
+``_build/``.  Rebuilds only what changed (by mtime against the sources and
+headers).
 """
 from __future__ import annotations
 
@@ -22,6 +25,9 @@ PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 REPO = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "lib", "libnutcracker_b200.so")
+CLI_SRC = os.path.join(PKG, "programs", "nutcracker.cpp")
+CLI = os.path.join(PKG, "bin", "nutcracker_b200")
+CXX = os.environ.get("CXX", "g++")
 BUILD = os.path.join(PKG, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -65,6 +71,15 @@ def build(verbose=False, force=False):
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)
             raise RuntimeError("link failed")
+    if os.path.exists(CLI_SRC) and (force or not os.path.exists(CLI) or
+                                    os.path.getmtime(CLI) < max(os.path.getmtime(CLI_SRC), os.path.getmtime(LIB))):
+        os.makedirs(os.path.dirname(CLI), exist_ok=True)
+        cmd = [CXX, "-std=c++17", "-O2", "-I", os.path.join(REPO, "include"), CLI_SRC,
+               "-L", os.path.dirname(LIB), "-lnutcracker_b200", "-Wl,-rpath,$ORIGIN/../lib", "-o", CLI]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError("building the command-line program failed")
     return LIB
 
 

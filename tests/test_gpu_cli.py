@@ -1,0 +1,54 @@
+"""Command-line program end to end on the GPU: the reference's README usage
+(`generator | nutcracker -n 4`) on the transverse-Ising operator that the
+reference's own generator emits (N=10, lambda=0.1), against the energies the
+reference's tests pin (tests/chain.cpp:300-305, 418-430; tests/stress.cpp:107-186).
+"""
+import os
+import subprocess
+
+import pytest
+import yaml
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(ROOT, "nutcracker-1_b200", "bin", "nutcracker_b200")
+TFIM = os.path.join(ROOT, "tests", "golden", "yaml", "transverse_ising_0.1_10.yaml")
+REF = [-10.022510957077, -8.213705725703, -8.188197237172, -8.148553771957]
+
+
+def run(args, stdin=b"", cwd=None):
+    return subprocess.run([CLI] + args, input=stdin, capture_output=True, cwd=cwd, timeout=600)
+
+
+def test_piped_four_levels_match_reference_energies():
+    r = run(["-n", "4"], stdin=open(TFIM, "rb").read())
+    assert r.returncode == 0, r.stderr
+    out = yaml.safe_load(r.stdout)
+    conf = out["Configuration"]
+    assert set(conf) == {"site convergence tolerance", "sweep convergence tolerance",
+                         "chain convergence tolerance", "sanity check threshold"}
+    levels = out["Energy levels"]
+    assert len(levels) == 4
+    for e, ref in zip(levels, REF):
+        assert abs(e - ref) <= 1e-9 * abs(ref), (levels, REF)
+
+
+def test_file_input_location_output_file_and_overwrite(tmp_path):
+    nested = "problem:\n  hamiltonian:\n" + "".join(
+        "    " + line + "\n" for line in open(TFIM).read().splitlines() if line and not line.startswith("---"))
+    (tmp_path / "in.yaml").write_text(nested)
+    (tmp_path / "nutcracker.cfg").write_text("chain-tolerance = 1e-10\n")
+    out = tmp_path / "out.yaml"
+    args = ["-f", str(tmp_path / "in.yaml"), "--input-location", "problem/hamiltonian", "-o", str(out)]
+    r = run(args, cwd=tmp_path)
+    assert r.returncode == 0, r.stderr
+    doc = yaml.safe_load(out.read_text())
+    assert float(doc["Configuration"]["chain convergence tolerance"]) == 1e-10   # "1e-10" is a YAML string
+    assert abs(doc["Energy levels"][0] - REF[0]) <= 1e-9 * abs(REF[0])
+    r = run(args, cwd=tmp_path)   # exists, no --output-overwrite
+    assert r.returncode == 0 and b"already exists." in r.stderr
+    r = run(args + ["--output-overwrite", "--precision", "1"], cwd=tmp_path)
+    assert r.returncode == 0, r.stderr
+    doc = yaml.safe_load(out.read_text())
+    assert abs(doc["Energy levels"][0] - REF[0]) <= 1e-9 * abs(REF[0])
