@@ -1,5 +1,5 @@
 /* C API of the B200 library with the reference's names and argument meaning
-   (includes/nutcracker.h; sources/c-interface/*.cpp).
+   (includes/nutcracker.h and the sources of sources/c-interface).
 
    Opaque objects are created by *_new / *_compile / *_deserialize and released
    with the matching *_free.  Functions that can fail return NULL (or leave
