@@ -453,18 +453,22 @@ void nc_server_free(nc_server* server);
    entries are a scalar (real), [re, im] or {real: re, imag: im}; the d*d data
    list is stored as written into the site's (d,d) column-major block.
    Host-only (no GPU needed). */
-typedef struct nc_yaml_operator nc_yaml_operator;
+typedef struct nc_parsed_operator nc_parsed_operator;
 /* Parses the first YAML document of `text` (`length` bytes).  `location`
    (NULL or "") selects the operator inside the document by slash-separated
    keys (--input-location).  NULL on error; nc_last_error() then holds the
    reference's message (e.g. "The 'from' index is too high. (4 > 3)"). */
-nc_yaml_operator* nc_yaml_read_operator(const char* text, size_t length, const char* location);
-uint32_t nc_yaml_operator_number_of_sites(const nc_yaml_operator* op);
+nc_parsed_operator* nc_yaml_read_operator(const char* text, size_t length, const char* location);
+uint32_t nc_parsed_operator_number_of_sites(const nc_parsed_operator* op);
 /* The chain's sites in order, ready for nc_chain_create / nc_server_submit;
-   valid until nc_yaml_operator_free. */
-const nc_operator_site* nc_yaml_operator_sites(const nc_yaml_operator* op);
-void nc_yaml_operator_free(nc_yaml_operator* op);
-/* Writes the operator in the same format (identical sites listed once, with
+   valid until nc_parsed_operator_free. */
+const nc_operator_site* nc_parsed_operator_sites(const nc_parsed_operator* op);
+void nc_parsed_operator_free(nc_parsed_operator* op);
+/* The protobuf operator format (OperatorBuffer of nutcracker.proto, 0-based
+   sequence; protobuf.cpp:41-99, 110-131): the input of the command-line
+   program's protobuf format.  NULL on error (nc_last_error()). */
+nc_parsed_operator* nc_protobuf_read_operator(const void* data, size_t length);
+/* Writes the operator in the YAML format (identical sites listed once, with
    the sequence); returns the text length and copies at most capacity-1 bytes
    plus a NUL into `out` (out may be NULL to query the length). */
 size_t nc_yaml_write_operator(uint32_t number_of_sites, const nc_operator_site* sites, char* out, size_t capacity);

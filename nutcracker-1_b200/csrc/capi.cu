@@ -23,6 +23,9 @@
 #include <string>
 #include <vector>
 
+#include "nc_abi_util.h"
+#include "nc_common.cuh"
+#include "nc_parsed_operator.h"
 #include "nutcracker.h"
 #include "nutcracker_b200.h"
 
@@ -707,6 +710,56 @@ std::vector<SitePtr> construct_operator(const std::vector<SitePtr>& unique, cons
     return out;
 }
 
+// OperatorBuffer (nutcracker.proto; protobuf.cpp:41-99): unique sites and the 0-based sequence.
+void parse_operator_buffer(const void* buffer, size_t size, std::vector<SitePtr>& unique, std::vector<uint32_t>& seq) {
+    if (!buffer && size) throw std::invalid_argument("null buffer");
+    const unsigned char* b = static_cast<const unsigned char*>(buffer);
+    Reader r{b, b + size};
+    while (!r.done()) {
+        const uint64_t tag = r.varint();
+        const unsigned field = (unsigned)(tag >> 3), wire = (unsigned)(tag & 7);
+        if (field == 1 && wire == 2) {
+            Reader m = r.sub();
+            auto s = std::make_shared<SiteData>();
+            uint64_t nnz = 0;
+            std::vector<double> data;
+            while (!m.done()) {
+                const uint64_t t = m.varint();
+                const unsigned f = (unsigned)(t >> 3), w = (unsigned)(t & 7);
+                if (f >= 1 && f <= 4 && w == 0) {
+                    const uint64_t v = m.varint();
+                    if (f == 1) nnz = v;
+                    else if (f == 2) s->d = (uint32_t)v;
+                    else if (f == 3) s->cl = (uint32_t)v;
+                    else s->cr = (uint32_t)v;
+                } else if (f == 5) {
+                    std::vector<double> d = read_doubles(m, w);
+                    data.insert(data.end(), d.begin(), d.end());
+                } else if (f == 6) {
+                    std::vector<uint32_t> i = read_uints(m, w);
+                    s->idx.insert(s->idx.end(), i.begin(), i.end());
+                } else {
+                    m.skip(w);
+                }
+            }
+            if (data.size() != 2 * nnz * s->d * s->d || s->idx.size() != 2 * nnz)
+                throw std::runtime_error("operator site buffer sizes do not match its number of matrices");
+            for (uint32_t k = 0; k < 2 * nnz; ++k) {
+                const uint32_t lim = (k % 2 == 0) ? s->cl : s->cr;
+                if (s->idx[k] < 1 || s->idx[k] > lim) throw std::runtime_error("operator site index out of range");
+            }
+            s->W.resize(data.size() / 2);
+            std::memcpy(s->W.data(), data.data(), data.size() * sizeof(double));
+            unique.push_back(s);
+        } else if (field == 2) {
+            std::vector<uint32_t> v = read_uints(r, wire);
+            seq.insert(seq.end(), v.begin(), v.end());
+        } else {
+            r.skip(wire);
+        }
+    }
+}
+
 std::vector<DataPtr> components_of(const NutcrackerMatrix* const* c, unsigned n) {
     std::vector<DataPtr> v;
     for (unsigned i = 0; i < n; ++i) v.push_back(need(c[i], "matrix").m);
@@ -939,56 +992,38 @@ NutcrackerSerialization* Nutcracker_Operator_serialize(NutcrackerOperator const*
 }
 NutcrackerOperator* Nutcracker_Operator_deserialize(uint32_t size, void const* buffer) {
     C_BEGIN
-    if (!buffer && size) throw std::invalid_argument("null buffer");
-    const unsigned char* b = static_cast<const unsigned char*>(buffer);
-    Reader r{b, b + size};
     std::vector<SitePtr> unique;
     std::vector<uint32_t> seq;
-    while (!r.done()) {
-        const uint64_t tag = r.varint();
-        const unsigned field = (unsigned)(tag >> 3), wire = (unsigned)(tag & 7);
-        if (field == 1 && wire == 2) {
-            Reader m = r.sub();
-            auto s = std::make_shared<SiteData>();
-            uint64_t nnz = 0;
-            std::vector<double> data;
-            while (!m.done()) {
-                const uint64_t t = m.varint();
-                const unsigned f = (unsigned)(t >> 3), w = (unsigned)(t & 7);
-                if (f >= 1 && f <= 4 && w == 0) {
-                    const uint64_t v = m.varint();
-                    if (f == 1) nnz = v;
-                    else if (f == 2) s->d = (uint32_t)v;
-                    else if (f == 3) s->cl = (uint32_t)v;
-                    else s->cr = (uint32_t)v;
-                } else if (f == 5) {
-                    std::vector<double> d = read_doubles(m, w);
-                    data.insert(data.end(), d.begin(), d.end());
-                } else if (f == 6) {
-                    std::vector<uint32_t> i = read_uints(m, w);
-                    s->idx.insert(s->idx.end(), i.begin(), i.end());
-                } else {
-                    m.skip(w);
-                }
-            }
-            if (data.size() != 2 * nnz * s->d * s->d || s->idx.size() != 2 * nnz)
-                throw std::runtime_error("operator site buffer sizes do not match its number of matrices");
-            for (uint32_t k = 0; k < 2 * nnz; ++k) {
-                const uint32_t lim = (k % 2 == 0) ? s->cl : s->cr;
-                if (s->idx[k] < 1 || s->idx[k] > lim) throw std::runtime_error("operator site index out of range");
-            }
-            s->W.resize(data.size() / 2);
-            std::memcpy(s->W.data(), data.data(), data.size() * sizeof(double));
-            unique.push_back(s);
-        } else if (field == 2) {
-            std::vector<uint32_t> v = read_uints(r, wire);
-            seq.insert(seq.end(), v.begin(), v.end());
-        } else {
-            r.skip(wire);
-        }
-    }
+    parse_operator_buffer(buffer, size, unique, seq);
     return new NutcrackerOperator{construct_operator(unique, seq)};
     C_END(nullptr)
+}
+
+// The protobuf input format of the command-line program (protobuf.cpp:110-131).
+nc_parsed_operator* nc_protobuf_read_operator(const void* data, size_t length) {
+    NC_ABI_BEGIN
+    std::vector<SitePtr> unique;
+    std::vector<uint32_t> seq;
+    try {
+        parse_operator_buffer(data, length, unique, seq);
+    } catch (const std::runtime_error& e) {
+        throw nc::Error(nc::NC_ERR_ARG, e.what());
+    }
+    auto op = std::make_unique<nc_parsed_operator>();
+    for (const SitePtr& u : unique) {
+        nc_parsed_operator::Site t;
+        t.d = u->d;
+        t.cl = u->cl;
+        t.cr = u->cr;
+        t.idx = u->idx;
+        t.W = u->W;
+        op->unique.push_back(std::move(t));
+    }
+    op->sequence = seq;
+    op->assemble();
+    return op.release();
+    NC_ABI_END
+    return nullptr;
 }
 
 // ---- serialization (serialization.cpp) ----

@@ -31,6 +31,7 @@
 #include "nc_abi_util.h"
 #include "nc_common.cuh"
 #include "nutcracker_b200.h"
+#include "nc_parsed_operator.h"
 
 using nc::g_status;
 
@@ -417,11 +418,7 @@ std::string fmt(const char* f, long long a) {
     return b;
 }
 
-struct UniqueSite {
-    uint32_t d = 0, cl = 0, cr = 0;
-    std::vector<uint32_t> idx;
-    std::vector<nc_complex> W;
-};
+using UniqueSite = nc_parsed_operator::Site;
 
 // OperatorSite reader (yaml.cpp:217-256).
 UniqueSite read_site(const YNode& node) {
@@ -459,15 +456,48 @@ UniqueSite read_site(const YNode& node) {
 
 }  // namespace
 
-struct nc_yaml_operator {
-    std::vector<UniqueSite> unique;
-    std::vector<uint32_t> sequence;   // 0-based indices into unique
-    std::vector<nc_operator_site> sites;
-};
+void nc_parsed_operator::assemble() {
+    // constructOperatorFrom (io.hpp:350-370)
+    if (sequence.empty()) fail("No operator sites were specified.");
+    for (size_t k = 0; k < sequence.size(); ++k) {
+        const uint32_t index = sequence[k];
+        if (index >= unique.size())
+            fail(fmt("When reading in an operator, a reference to the non-existent operator site number %lld "
+                     "appeared in the sequence.", (long long)index));
+        const UniqueSite& u = unique[index];
+        if (k == 0) {
+            if (u.cl != 1) fail(fmt("The left dimension of the left-most site must be one but instead is %lld.", u.cl));
+        } else {
+            const UniqueSite& prev = unique[sequence[k - 1]];
+            if (u.cl != prev.cr) {
+                char b[256];
+                std::snprintf(b, sizeof b,
+                              "The left dimension (%u) of site %zu does not match the right dimension (%u) of site "
+                              "%zu.  (%u != %u)",
+                              u.cl, k - 1, prev.cr, k, u.cl, prev.cr);
+                fail(b);
+            }
+        }
+    }
+    const UniqueSite& last = unique[sequence.back()];
+    if (last.cr != 1) fail(fmt("The right dimension of the right-most site must be one but instead is %lld.", last.cr));
+    sites.clear();
+    for (uint32_t index : sequence) {
+        const UniqueSite& u = unique[index];
+        nc_operator_site s;
+        s.physical_dimension = u.d;
+        s.left_dimension = u.cl;
+        s.right_dimension = u.cr;
+        s.number_of_matrices = (uint32_t)(u.idx.size() / 2);
+        s.indices = u.idx.data();
+        s.matrices = u.W.data();
+        sites.push_back(s);
+    }
+}
 
 extern "C" {
 
-nc_yaml_operator* nc_yaml_read_operator(const char* text, size_t length, const char* location) {
+nc_parsed_operator* nc_yaml_read_operator(const char* text, size_t length, const char* location) {
     NC_ABI_BEGIN
     NC_ARG(text != nullptr, "nc_yaml_read_operator: null text");
     Parser parser(std::string(text, length));
@@ -487,7 +517,7 @@ nc_yaml_operator* nc_yaml_read_operator(const char* text, size_t length, const c
             if (!node) fail("No such location " + loc + ".");
         }
     }
-    auto op = std::make_unique<nc_yaml_operator>();
+    auto op = std::make_unique<nc_parsed_operator>();
     const YNode* sites = node ? node->get("sites") : nullptr;
     if (sites && sites->kind == YNode::Seq)
         for (const YPtr& s : sites->seq) {
@@ -499,53 +529,19 @@ nc_yaml_operator* nc_yaml_read_operator(const char* text, size_t length, const c
     const YNode* seq = node ? node->get("sequence") : nullptr;
     if (seq && seq->kind == YNode::Seq)
         for (const YPtr& e : seq->seq) op->sequence.push_back((uint32_t)(as_integer(e.get(), "sequence") - 1));
-    // constructOperatorFrom (io.hpp:350-370)
-    if (op->sequence.empty()) fail("No operator sites were specified.");
-    for (size_t k = 0; k < op->sequence.size(); ++k) {
-        const uint32_t index = op->sequence[k];
-        if (index >= op->unique.size())
-            fail(fmt("When reading in an operator, a reference to the non-existent operator site number %lld "
-                     "appeared in the sequence.", (long long)index));
-        const UniqueSite& u = op->unique[index];
-        if (k == 0) {
-            if (u.cl != 1) fail(fmt("The left dimension of the left-most site must be one but instead is %lld.", u.cl));
-        } else {
-            const UniqueSite& prev = op->unique[op->sequence[k - 1]];
-            if (u.cl != prev.cr) {
-                char b[256];
-                std::snprintf(b, sizeof b,
-                              "The left dimension (%u) of site %zu does not match the right dimension (%u) of site "
-                              "%zu.  (%u != %u)",
-                              u.cl, k - 1, prev.cr, k, u.cl, prev.cr);
-                fail(b);
-            }
-        }
-    }
-    const UniqueSite& last = op->unique[op->sequence.back()];
-    if (last.cr != 1) fail(fmt("The right dimension of the right-most site must be one but instead is %lld.", last.cr));
-    for (uint32_t index : op->sequence) {
-        const UniqueSite& u = op->unique[index];
-        nc_operator_site s;
-        s.physical_dimension = u.d;
-        s.left_dimension = u.cl;
-        s.right_dimension = u.cr;
-        s.number_of_matrices = (uint32_t)(u.idx.size() / 2);
-        s.indices = u.idx.data();
-        s.matrices = u.W.data();
-        op->sites.push_back(s);
-    }
+    op->assemble();
     return op.release();
     NC_ABI_END
     return nullptr;
 }
 
-uint32_t nc_yaml_operator_number_of_sites(const nc_yaml_operator* op) { return op ? (uint32_t)op->sites.size() : 0; }
+uint32_t nc_parsed_operator_number_of_sites(const nc_parsed_operator* op) { return op ? (uint32_t)op->sites.size() : 0; }
 
-const nc_operator_site* nc_yaml_operator_sites(const nc_yaml_operator* op) {
+const nc_operator_site* nc_parsed_operator_sites(const nc_parsed_operator* op) {
     return op && !op->sites.empty() ? op->sites.data() : nullptr;
 }
 
-void nc_yaml_operator_free(nc_yaml_operator* op) { delete op; }
+void nc_parsed_operator_free(nc_parsed_operator* op) { delete op; }
 
 size_t nc_yaml_write_operator(uint32_t number_of_sites, const nc_operator_site* sites, char* out, size_t capacity) {
     // Operator emitter (yaml.cpp:186-206, 257-306): unique sites (here by

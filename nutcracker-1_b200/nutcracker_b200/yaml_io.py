@@ -18,11 +18,11 @@ from .operators import OperatorSite
 
 lib.nc_yaml_read_operator.restype = ct.c_void_p
 lib.nc_yaml_read_operator.argtypes = [ct.c_char_p, ct.c_size_t, ct.c_char_p]
-lib.nc_yaml_operator_number_of_sites.restype = ct.c_uint32
-lib.nc_yaml_operator_number_of_sites.argtypes = [ct.c_void_p]
-lib.nc_yaml_operator_sites.restype = ct.POINTER(nc_operator_site)
-lib.nc_yaml_operator_sites.argtypes = [ct.c_void_p]
-lib.nc_yaml_operator_free.argtypes = [ct.c_void_p]
+lib.nc_parsed_operator_number_of_sites.restype = ct.c_uint32
+lib.nc_parsed_operator_number_of_sites.argtypes = [ct.c_void_p]
+lib.nc_parsed_operator_sites.restype = ct.POINTER(nc_operator_site)
+lib.nc_parsed_operator_sites.argtypes = [ct.c_void_p]
+lib.nc_parsed_operator_free.argtypes = [ct.c_void_p]
 lib.nc_yaml_write_operator.restype = ct.c_size_t
 lib.nc_yaml_write_operator.argtypes = [ct.c_uint32, ct.POINTER(nc_operator_site), ct.c_char_p, ct.c_size_t]
 
@@ -36,8 +36,8 @@ def read_operator(text, location=None):
         _check()
         raise NutcrackerError(-1, "nc_yaml_read_operator failed")
     try:
-        n = lib.nc_yaml_operator_number_of_sites(h)
-        arr = lib.nc_yaml_operator_sites(h)
+        n = lib.nc_parsed_operator_number_of_sites(h)
+        arr = lib.nc_parsed_operator_sites(h)
         sites = []
         for i in range(n):
             s = arr[i]
@@ -52,7 +52,7 @@ def read_operator(text, location=None):
             sites.append(OperatorSite(d, s.left_dimension, s.right_dimension, idx.astype(np.uint32), W))
         return sites
     finally:
-        lib.nc_yaml_operator_free(h)
+        lib.nc_parsed_operator_free(h)
 
 
 def write_operator(sites):

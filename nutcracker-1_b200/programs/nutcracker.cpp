@@ -33,6 +33,7 @@
 #include <iomanip>
 #include <iostream>
 #include <map>
+#include <memory>
 #include <sstream>
 #include <stdexcept>
 #include <string>
@@ -206,8 +207,10 @@ void print_help_and_exit() {
 }
 
 void print_formats_and_exit() {
-    std::cerr << "The recognized input format types are:\n  - yaml: YAML format\n\n"
-                 "The recognized output format types are:\n  - yaml: YAML format\n\n";
+    std::cerr << "The recognized input format types are:\n  - protobuf: Google Protocol Buffers format\n"
+                 "  - yaml: YAML format\n\n"
+                 "The recognized output format types are:\n  - protobuf: Google Protocol Buffers format\n"
+                 "  - yaml: YAML format\n\n";
     std::exit(1);
 }
 
@@ -217,17 +220,30 @@ void print_modes_and_exit() {
     std::exit(1);
 }
 
-// resolveAndCheckFormat (io.hpp:389-418) with yaml as the only (and default)
-// format: it reads and writes pipes; only the input supports locations; the
-// output supports no states.
-void resolve_format(const Values& v, const char* type, const char* format_key, const char* location_key) {
+// resolveAndCheckFormat (io.hpp:389-418) over the two formats (yaml.cpp:145-148,
+// protobuf.cpp:191-194): both read and write pipes, the named format wins,
+// else the file extension (.yaml, .prb), else yaml; only the YAML input
+// supports locations.
+std::string resolve_format(const Values& v, const char* type, const char* format_key, const char* file_key,
+                           const char* location_key) {
+    std::string format = "yaml";
     auto f = v.find(format_key);
-    if (f != v.end() && f->second != "yaml")
-        throw FormatError(f->second + " is not a recognized/supported " + type + " format type.\n\nThe recognized " +
-                          type + " format types are:\n  - yaml\n\nRun Nutcracker with the --help-formats option for "
-                          "more informaton about supported formats.");
-    if (std::string(type) == "output" && v.count(location_key))
-        throw FormatError("The output format type yaml does not support locations.");
+    if (f != v.end()) {
+        if (f->second != "yaml" && f->second != "protobuf")
+            throw FormatError(f->second + " is not a recognized/supported " + type + " format type.\n\nThe "
+                              "recognized " + type + " format types are:\n  - protobuf\n  - yaml\n\nRun Nutcracker "
+                              "with the --help-formats option for more informaton about supported formats.");
+        format = f->second;
+    } else if (v.count(file_key)) {
+        const std::string& name = v.at(file_key);
+        const size_t dot = name.rfind('.'), slash = name.rfind('/');
+        if (dot != std::string::npos && (slash == std::string::npos || dot > slash) && name.substr(dot + 1) == "prb")
+            format = "protobuf";
+    }
+    const bool locations = std::string(type) == "input" && format == "yaml";
+    if (v.count(location_key) && !locations)
+        throw FormatError("The " + std::string(type) + " format type " + format + " does not support locations.");
+    return format;
 }
 
 std::string read_all(std::istream& in) {
@@ -245,10 +261,55 @@ unsigned digits_of_precision(double tolerance) {   // utilities.cpp:92-95
     return estimated > 0 ? (unsigned)estimated : 1;
 }
 
+// ---- protobuf output: SimulationResultsBuffer of nutcracker.proto ----
+void pb_varint(std::string& o, uint64_t v) {
+    while (v >= 0x80) {
+        o.push_back((char)(v | 0x80));
+        v >>= 7;
+    }
+    o.push_back((char)v);
+}
+void pb_uint(std::string& o, unsigned field, uint64_t v) {
+    pb_varint(o, (uint64_t)field << 3);
+    pb_varint(o, v);
+}
+void pb_double(std::string& o, unsigned field, double x) {
+    pb_varint(o, ((uint64_t)field << 3) | 1);
+    char b[8];
+    std::memcpy(b, &x, 8);
+    o.append(b, 8);
+}
+void pb_bytes(std::string& o, unsigned field, const std::string& b) {
+    pb_varint(o, ((uint64_t)field << 3) | 2);
+    pb_varint(o, b.size());
+    o += b;
+}
+
+// StateBuffer of the chain's state with its centre on site 0 (protobuf.cpp:86-104).
+std::string state_buffer(nc_chain* chain, uint32_t n) {
+    if (nc_chain_move_to(chain, 0) != 0) Library::fail();
+    std::string out;
+    for (uint32_t i = 0; i < n; ++i) {
+        uint32_t dims[3];
+        if (nc_chain_get_site(chain, i, nullptr, dims) != 0) Library::fail();
+        std::vector<nc_complex> w((size_t)dims[0] * dims[1] * dims[2]);
+        if (nc_chain_get_site(chain, i, w.data(), dims) != 0) Library::fail();
+        std::string m;
+        pb_uint(m, 1, i == 0 ? 0 : 2);   // MIDDLE, then RIGHT
+        pb_uint(m, 2, dims[2]);
+        pb_uint(m, 3, dims[1]);
+        pb_uint(m, 4, dims[0]);
+        pb_bytes(m, 5, std::string(reinterpret_cast<const char*>(w.data()), w.size() * sizeof(nc_complex)));
+        pb_bytes(out, 1, m);
+    }
+    return out;
+}
+
 int run(const Values& v) {
-    resolve_format(v, "input", "input-format", "input-location");
-    resolve_format(v, "output", "output-format", "output-location");
-    if (to_flag(v, "output-states")) throw FormatError("Output format yaml does not support outputing states.");
+    const std::string in_format = resolve_format(v, "input", "input-format", "input-file", "input-location");
+    const std::string out_format = resolve_format(v, "output", "output-format", "output-file", "output-location");
+    if (to_flag(v, "output-states") && out_format == "yaml")
+        throw FormatError("Output format yaml does not support outputing states.");
 
     nc_chain_options o;
     nc_chain_options_init(&o);
@@ -272,53 +333,68 @@ int run(const Values& v) {
     } else {
         text = read_all(std::cin);
     }
-    const char* location = v.count("input-location") ? v.at("input-location").c_str() : nullptr;
-    nc_yaml_operator* op = nc_yaml_read_operator(text.data(), text.size(), location);
+    nc_parsed_operator* op;
+    if (in_format == "protobuf") {
+        op = nc_protobuf_read_operator(text.data(), text.size());
+    } else {
+        const char* location = v.count("input-location") ? v.at("input-location").c_str() : nullptr;
+        op = nc_yaml_read_operator(text.data(), text.size(), location);
+    }
     if (!op) Library::fail();
-    nc_chain* chain = nc_chain_create(nc_yaml_operator_number_of_sites(op), nc_yaml_operator_sites(op), &o);
-    nc_yaml_operator_free(op);
+    const uint32_t n_sites = nc_parsed_operator_number_of_sites(op);
+    nc_chain* chain = nc_chain_create(n_sites, nc_parsed_operator_sites(op), &o);
+    nc_parsed_operator_free(op);
     if (!chain) Library::fail();
+    std::unique_ptr<nc_chain, void (*)(nc_chain*)> guard(chain, nc_chain_free);
 
-    // the YAML outputter (yaml.cpp:106-143)
+    // the outputters (yaml.cpp:106-143; protobuf.cpp:132-170, which checks no
+    // existing file and writes everything at the end)
+    const bool yaml = out_format == "yaml";
     std::ofstream file;
     if (v.count("output-file")) {
         const std::string& name = v.at("output-file");
-        if (!to_flag(v, "output-overwrite") && std::ifstream(name).good()) {
-            nc_chain_free(chain);
+        if (yaml && !to_flag(v, "output-overwrite") && std::ifstream(name).good())
             throw std::runtime_error("The output filename " + name + " already exists.");
-        }
-        file.open(name);
-        if (!file) {
-            nc_chain_free(chain);
-            throw std::runtime_error("cannot open the output file " + name);
-        }
+        file.open(name, std::ios::binary);
+        if (!file) throw std::runtime_error("cannot open the output file " + name);
     }
     std::ostream& out = v.count("output-file") ? static_cast<std::ostream&>(file) : std::cout;
-    out << "Configuration:\n"
-        << "  site convergence tolerance: " << o.site_convergence_threshold << "\n"
-        << "  sweep convergence tolerance: " << o.sweep_convergence_threshold << "\n"
-        << "  chain convergence tolerance: " << o.chain_convergence_threshold << "\n"
-        << "  sanity check threshold: " << o.sanity_check_threshold << "\n"
-        << "Energy levels:\n";
-    out.flush();
-    const unsigned digits = digits_of_precision(o.chain_convergence_threshold);
-
-    // solveForMultipleLevels (chain.cpp:301-310), one line per optimised level
-    for (unsigned k = 0; k < levels; ++k) {
-        if (k > 0 && (nc_chain_construct_and_add_projector_from_state(chain) != 0 || nc_chain_reset(chain) != 0)) {
-            nc_chain_free(chain);
-            Library::fail();
-        }
-        double e = 0;
-        if (nc_chain_optimize_chain(chain) != 0 || nc_chain_get_energy(chain, &e) != 0) {
-            const std::string msg = nc_last_error();
-            nc_chain_free(chain);
-            throw std::runtime_error(msg);
-        }
-        out << "  - " << std::setprecision(digits) << e << "\n";
+    if (yaml) {
+        out << "Configuration:\n"
+            << "  site convergence tolerance: " << o.site_convergence_threshold << "\n"
+            << "  sweep convergence tolerance: " << o.sweep_convergence_threshold << "\n"
+            << "  chain convergence tolerance: " << o.chain_convergence_threshold << "\n"
+            << "  sanity check threshold: " << o.sanity_check_threshold << "\n"
+            << "Energy levels:\n";
         out.flush();
     }
-    nc_chain_free(chain);
+    const unsigned digits = digits_of_precision(o.chain_convergence_threshold);
+    std::string results;
+
+    // solveForMultipleLevels (chain.cpp:301-310), one result per optimised level
+    for (unsigned k = 0; k < levels; ++k) {
+        if (k > 0 && (nc_chain_construct_and_add_projector_from_state(chain) != 0 || nc_chain_reset(chain) != 0))
+            Library::fail();
+        double e = 0;
+        if (nc_chain_optimize_chain(chain) != 0 || nc_chain_get_energy(chain, &e) != 0) Library::fail();
+        if (yaml) {
+            out << "  - " << std::setprecision(digits) << e << "\n";
+            out.flush();
+        } else {
+            std::string solution;
+            pb_double(solution, 1, e);
+            pb_bytes(solution, 2, state_buffer(chain, n_sites));   // states are always written, as the reference does
+            pb_bytes(results, 1, solution);
+        }
+    }
+    if (!yaml) {
+        pb_double(results, 2, o.sanity_check_threshold);
+        pb_double(results, 3, o.site_convergence_threshold);
+        pb_double(results, 4, o.sweep_convergence_threshold);
+        pb_double(results, 5, o.chain_convergence_threshold);
+        out.write(results.data(), (std::streamsize)results.size());
+        out.flush();
+    }
     return 0;
 }
 

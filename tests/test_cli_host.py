@@ -21,7 +21,8 @@ def test_help_listings_exit_1():
     r = run(["--help-modes"])
     assert r.returncode == 1 and b"'<v' - least value" in r.stderr and b"'>m' - largest magnitude" in r.stderr
     r = run(["--help-formats"])
-    assert r.returncode == 1 and b"The recognized input format types are:\n  - yaml: YAML format" in r.stderr
+    assert r.returncode == 1 and (b"The recognized input format types are:\n  - protobuf: Google Protocol Buffers "
+                                  b"format\n  - yaml: YAML format") in r.stderr
     r = run(["--help"])
     assert r.returncode == 1 and b"--number-of-levels [ -n ]" in r.stderr and b"site-tolerance = 1e-10" in r.stderr
 
@@ -42,6 +43,8 @@ def test_option_errors_exit_255(args, message):
     (["--input-format", "hdf"], b"hdf is not a recognized/supported input format type."),
     (["--output-format", "text"], b"text is not a recognized/supported output format type."),
     (["--output-location", "a/b"], b"The output format type yaml does not support locations."),
+    (["--input-format", "protobuf", "--input-location", "a"], b"The input format type protobuf does not support locations."),
+    (["-f", "in.prb", "--input-location", "a"], b"The input format type protobuf does not support locations."),
     (["--output-states"], b"Output format yaml does not support outputing states."),
 ])
 def test_format_errors_exit_255(args, message):
@@ -59,6 +62,20 @@ def test_operator_errors_are_reported(tmp_path):
     assert b"No such location nowhere." in r.stderr
     r = run(["-f", str(tmp_path / "missing.yaml")])
     assert b"cannot open the input file" in r.stderr
+
+
+def test_protobuf_input_errors(tmp_path):
+    from nutcracker_b200 import capi
+    b = capi.OperatorBuilder([2] * 3)
+    b.add_term(capi.OperatorTerm.global_external_field(capi.Matrix.pauli("Z")))
+    data = b.compile().serialize()
+    r = run(["--input-format", "protobuf"], stdin=data[:-2])
+    assert r.returncode == 0 and b"truncated" in r.stderr
+    (tmp_path / "op.prb").write_bytes(data[:-2])
+    r = run(["-f", str(tmp_path / "op.prb")])
+    assert b"truncated" in r.stderr
+    r = run(["--input-format", "protobuf"], stdin=b"")
+    assert b"No operator sites were specified." in r.stderr
 
 
 def test_configuration_file(tmp_path):

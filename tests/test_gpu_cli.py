@@ -52,3 +52,32 @@ def test_file_input_location_output_file_and_overwrite(tmp_path):
     assert r.returncode == 0, r.stderr
     doc = yaml.safe_load(out.read_text())
     assert abs(doc["Energy levels"][0] - REF[0]) <= 1e-9 * abs(REF[0])
+
+
+def test_protobuf_formats_end_to_end(tmp_path):
+    """Operator in as an OperatorBuffer, results out as a SimulationResultsBuffer
+    (nutcracker.proto) with an eigenvector state per level."""
+    import struct
+
+    from nutcracker_b200 import capi
+    from test_capi_host import _fields
+
+    b = capi.OperatorBuilder([2] * 10)
+    b.add_term(capi.OperatorTerm.transverse_ising_field(capi.Matrix.pauli("Z"), 0.1 * capi.Matrix.pauli("X"),
+                                                        capi.Matrix.pauli("X")))
+    op = b.compile()
+    (tmp_path / "op.prb").write_bytes(op.serialize())
+    out = tmp_path / "res.prb"
+    r = run(["-f", str(tmp_path / "op.prb"), "-o", str(out), "-n", "2"])
+    assert r.returncode == 0, r.stderr
+    fields = _fields(out.read_bytes())
+    solutions = [v for f, w, v in fields if f == 1]
+    thresholds = {f: struct.unpack("<d", v)[0] for f, w, v in fields if f in (2, 3, 4, 5)}
+    assert len(solutions) == 2 and set(thresholds) == {2, 3, 4, 5}
+    for k, sol in enumerate(solutions):
+        sf = {f: v for f, w, v in _fields(sol)}
+        e = struct.unpack("<d", sf[1])[0]
+        assert abs(e - REF[k]) <= 1e-9 * abs(REF[k])
+        state = capi.State.deserialize(sf[2])
+        assert abs(state.overlap(state) - 1) < 1e-10
+        assert abs(state.expectation(op) - e) < 1e-8 * abs(e)
