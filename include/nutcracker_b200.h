@@ -387,6 +387,22 @@ int nc_chain_footprint_bytes(uint32_t number_of_sites, const nc_operator_site* s
 int nc_chain_set_precision(nc_chain* chain, uint32_t precision);
 int nc_chain_increase_bandwidth_dimension(nc_chain* chain, uint32_t new_dimension); /* chain.cpp:75-122 */
 int nc_chain_construct_and_add_projector_from_state(nc_chain* chain);  /* chain.cpp:63-73 */
+/* Signals (base_chain.hpp:54-60, chain.hpp:151): `fn` runs on the calling
+   thread when the event happens, in connection order; it may call the
+   nc_chain_* query functions.  value: the site solve's H_eff products
+   (success), the failure kind (failure), the sweep count (sweep performed),
+   else 0.  nc_chain_connect returns a connection id (> 0) or -1. */
+enum {
+    NC_SIGNAL_OPTIMIZE_SITE_SUCCESS = 1,
+    NC_SIGNAL_OPTIMIZE_SITE_FAILURE = 2,
+    NC_SIGNAL_SWEEP_PERFORMED = 3,
+    NC_SIGNAL_SWEEPS_CONVERGED = 4,
+    NC_SIGNAL_CHAIN_OPTIMIZED = 5,
+    NC_SIGNAL_CHAIN_RESET = 6
+};
+typedef void (*nc_chain_signal_fn)(nc_chain* chain, int signal, int64_t value, void* user);
+int64_t nc_chain_connect(nc_chain* chain, int signal, nc_chain_signal_fn fn, void* user);
+int nc_chain_disconnect(nc_chain* chain, int64_t connection);
 /* solveForEigenvalues (chain.cpp:292-310): `eigenvalues` receives n levels. */
 int nc_chain_solve_for_eigenvalues(nc_chain* chain, uint32_t number_of_levels, double* eigenvalues);
 int nc_chain_move_to(nc_chain* chain, uint32_t site);        /* chain.cpp:124-133 */

@@ -161,6 +161,23 @@ struct Chain {
     bool optimized = false;
     uint64_t seed_counter = 0;
     ChainStats stats;
+    // Signals (base_chain.hpp:54-60, chain.hpp:151): host callbacks run on the
+    // calling thread, in connection order, when the event happens.
+    struct Slot {
+        int64_t id;
+        int signal;
+        nc_chain_signal_fn fn;
+        void* user;
+    };
+    std::vector<Slot> slots;
+    int64_t next_slot = 1;
+    nc_chain* handle = nullptr;
+    int last_matvecs = 0;
+    void emit(int signal, int64_t value) {
+        const std::vector<Slot> now = slots;   // callbacks may connect or disconnect
+        for (const Slot& s : now)
+            if (s.signal == signal) s.fn(handle, signal, value, s.user);
+    }
     // precision form: 0 = FP64 sweeps, 1 = 3xTF32 tensor-core products
     int prec = 0;
     int free_sweeps = 0;   // sweeps still exempt from the regression check (after a precision hand-over)
@@ -398,6 +415,7 @@ struct Chain {
         if (std::fabs(last_expectation.y) / scale > imag_tol)
             throw Error(NC_ERR_NUMERIC, "initial chain energy is not real");
         energy = e;
+        emit(NC_SIGNAL_CHAIN_RESET, 0);   // chain.cpp:236
     }
 
     uint64_t next_seed() { return opt.seed * 0x9E3779B97F4A7C15ull + (++seed_counter) * 0xD1B54A32D192ED03ull; }
@@ -486,6 +504,7 @@ struct Chain {
                                      (int)opt.maximum_number_of_iterations, site[cur].p, spare_a.p, &ev, &normal, &es,
                                      mixed);
         stats.matvecs += es.matvecs;
+        last_matvecs = es.matvecs;
         stats.site_solves++;
         const double sanity = prec ? std::max(opt.sanity_check_threshold, kMixedSanity) : opt.sanity_check_threshold;
         int failure = 0;
@@ -528,7 +547,12 @@ struct Chain {
     }
 
     int optimize_site() {
+        last_matvecs = 0;
         int f = optimize_site_once();
+        // base_chain.cpp:104-109: success carries the solver's iteration count
+        // (here its H_eff products), failure the failure kind
+        if (f) emit(NC_SIGNAL_OPTIMIZE_SITE_FAILURE, f);
+        else emit(NC_SIGNAL_OPTIMIZE_SITE_SUCCESS, last_matvecs);
         if (f && opt.strict) throw Error(NC_ERR_NUMERIC, "site optimisation failed (code " + std::to_string(f) + ")");
         return f;
     }
@@ -546,6 +570,7 @@ struct Chain {
         }
         if (free_sweeps > 0) --free_sweeps;
         stats.sweeps++;
+        emit(NC_SIGNAL_SWEEP_PERFORMED, (int64_t)stats.sweeps);   // chain.cpp:162
     }
 
     void sweep_until_converged() {
@@ -604,6 +629,7 @@ struct Chain {
             prev = now;
             now = energy;
         }
+        emit(NC_SIGNAL_SWEEPS_CONVERGED, 0);   // base_chain.cpp:122
     }
 
     void increase_bandwidth_dimension(int new_b) {
@@ -666,6 +692,7 @@ struct Chain {
             prev = now;
             now = energy;
         }
+        emit(NC_SIGNAL_CHAIN_OPTIMIZED, 0);   // base_chain.cpp:78
     }
 
     void construct_and_add_projector_from_state() {
@@ -829,6 +856,7 @@ nc_chain* nc_chain_create(uint32_t number_of_sites, const nc_operator_site* site
     auto h = new nc_chain;
     try {
         h->impl = std::make_unique<Chain>(Context::get(), (int)number_of_sites, d.data(), to_options(options));
+        h->impl->handle = h;
     } catch (...) {
         delete h;
         throw;
@@ -850,6 +878,27 @@ void nc_chain_free(nc_chain* c) { delete c; }
     return g_status;
 
 int nc_chain_reset(nc_chain* c) { NC_CHAIN_CALL(ch.reset()) }
+
+int64_t nc_chain_connect(nc_chain* c, int signal, nc_chain_signal_fn fn, void* user) {
+    NC_ABI_BEGIN
+    NC_ARG(c && c->impl, "null chain");
+    NC_ARG(fn != nullptr, "null callback");
+    NC_ARG(signal >= NC_SIGNAL_OPTIMIZE_SITE_SUCCESS && signal <= NC_SIGNAL_CHAIN_RESET, "unknown signal");
+    Chain& ch = *c->impl;
+    const int64_t id = ch.next_slot++;
+    ch.slots.push_back(Chain::Slot{id, signal, fn, user});
+    return id;
+    NC_ABI_END
+    return -1;
+}
+
+int nc_chain_disconnect(nc_chain* c, int64_t id) {
+    NC_CHAIN_CALL({
+        auto it = std::find_if(ch.slots.begin(), ch.slots.end(), [&](const Chain::Slot& s) { return s.id == id; });
+        NC_ARG(it != ch.slots.end(), "no such connection");
+        ch.slots.erase(it);
+    })
+}
 
 int nc_chain_set_state(nc_chain* c, const uint32_t* bond_dimensions, const nc_complex* const* sites) {
     NC_CHAIN_CALL({

@@ -79,6 +79,13 @@ lib.nc_chain_move_to.argtypes = [ct.c_void_p, ct.c_uint32]
 lib.nc_chain_set_precision.argtypes = [ct.c_void_p, ct.c_uint32]
 lib.nc_chain_solve_for_eigenvalues.argtypes = [ct.c_void_p, ct.c_uint32, ct.POINTER(ct.c_double)]
 lib.nc_chain_solve_levels_at_bandwidth.argtypes = [ct.c_void_p, ct.c_uint32, ct.POINTER(ct.c_double)]
+SIGNAL_FN = ct.CFUNCTYPE(None, ct.c_void_p, ct.c_int, ct.c_int64, ct.c_void_p)
+lib.nc_chain_connect.restype = ct.c_int64
+lib.nc_chain_connect.argtypes = [ct.c_void_p, ct.c_int, SIGNAL_FN, ct.c_void_p]
+lib.nc_chain_disconnect.argtypes = [ct.c_void_p, ct.c_int64]
+# signal numbers (include/nutcracker_b200.h)
+SIGNALS = {"optimize_site_success": 1, "optimize_site_failure": 2, "sweep_performed": 3,
+           "sweeps_converged": 4, "chain_optimized": 5, "chain_reset": 6}
 lib.nc_chain_get_energy.argtypes = [ct.c_void_p, ct.POINTER(ct.c_double)]
 lib.nc_chain_compute_expectation_value.argtypes = [ct.c_void_p, ct.POINTER(ct.c_double)]
 lib.nc_chain_get_info.argtypes = [ct.c_void_p, ct.POINTER(nc_chain_info)]
@@ -144,6 +151,21 @@ class Chain:
         if st != 0:
             _check()
             raise NutcrackerError(st, "chain call failed")
+
+    # -- signals (base_chain.hpp:54-60, chain.hpp:151) ------------------------
+    def connect(self, signal, callback):
+        """Call ``callback(value)`` on ``signal`` (a key of SIGNALS); returns a
+        connection id for ``disconnect``."""
+        fn = SIGNAL_FN(lambda _h, _s, value, _u: callback(value))
+        cid = lib.nc_chain_connect(self._h, SIGNALS[signal], fn, None)
+        if cid < 0:
+            _check()
+        self.__dict__.setdefault("_slots", {})[cid] = fn   # keep the trampoline alive
+        return cid
+
+    def disconnect(self, cid):
+        self._call(lib.nc_chain_disconnect, ct.c_int64(cid))
+        self._slots.pop(cid, None)
 
     # -- reference API ----------------------------------------------------
     def reset(self):

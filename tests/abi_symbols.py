@@ -14,7 +14,7 @@ def declared_symbols():
         src = re.sub(r"//[^\n]*", "", src)
         for m in re.finditer(r"^[A-Za-z_][\w\s\*]*?\b([A-Za-z_]\w*)\s*\(", src, re.M):
             name = m.group(1)
-            if name in ("if", "while", "for", "return", "sizeof"):
+            if name in ("if", "while", "for", "return", "sizeof") or m.group(0).startswith("typedef"):
                 continue
             names.append(name)
     return names
