@@ -387,6 +387,14 @@ int nc_chain_footprint_bytes(uint32_t number_of_sites, const nc_operator_site* s
 int nc_chain_set_precision(nc_chain* chain, uint32_t precision);
 int nc_chain_increase_bandwidth_dimension(nc_chain* chain, uint32_t new_dimension); /* chain.cpp:75-122 */
 int nc_chain_construct_and_add_projector_from_state(nc_chain* chain);  /* chain.cpp:63-73 */
+/* Checkpoint / resume: the chain's state (centre moved to site 0) in the
+   StateBuffer layout of nutcracker.proto (first site MIDDLE, the rest RIGHT).
+   nc_chain_serialize_state returns the byte count and writes the bytes when
+   capacity suffices (out may be NULL to query); 0 on error.
+   nc_chain_deserialize_state resets the chain to such a state (its own sites'
+   physical dimensions) and recomputes the environments and the energy. */
+size_t nc_chain_serialize_state(nc_chain* chain, void* out, size_t capacity);
+int nc_chain_deserialize_state(nc_chain* chain, const void* data, size_t length);
 /* Signals (base_chain.hpp:54-60, chain.hpp:151): `fn` runs on the calling
    thread when the event happens, in connection order; it may call the
    nc_chain_* query functions.  value: the site solve's H_eff products

@@ -1337,3 +1337,63 @@ NutcrackerStateTerm* Nutcracker_StateTerm_create_W(NutcrackerVector const* commo
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Checkpoint and resume of a chain's state in the StateBuffer layout
+// (nutcracker.proto; the state the reference's protobuf outputter writes,
+// protobuf.cpp:101-104): the centre moved to site 0, then every site.
+// ---------------------------------------------------------------------------
+extern "C" {
+
+size_t nc_chain_serialize_state(nc_chain* chain, void* out, size_t capacity) {
+    NC_ABI_BEGIN
+    NC_ARG(chain != nullptr, "null chain");
+    nc_chain_info info;
+    if (nc_chain_get_info(chain, &info) != 0 || nc_chain_move_to(chain, 0) != 0)
+        throw nc::Error(nc_last_status(), nc_last_error());
+    std::string buf;
+    for (uint32_t i = 0; i < info.number_of_sites; ++i) {
+        uint32_t dims[3];
+        if (nc_chain_get_site(chain, i, nullptr, dims) != 0) throw nc::Error(nc_last_status(), nc_last_error());
+        std::vector<nc_complex> w((size_t)dims[0] * dims[1] * dims[2]);
+        if (nc_chain_get_site(chain, i, w.data(), dims) != 0) throw nc::Error(nc_last_status(), nc_last_error());
+        std::string m;
+        put_uint(m, 1, i == 0 ? 0 : 2);
+        put_uint(m, 2, dims[2]);
+        put_uint(m, 3, dims[1]);
+        put_uint(m, 4, dims[0]);
+        put_packed_doubles(m, 5, w);
+        put_bytes(buf, 1, m);
+    }
+    if (out && capacity >= buf.size()) std::memcpy(out, buf.data(), buf.size());
+    return buf.size();
+    NC_ABI_END
+    return 0;
+}
+
+int nc_chain_deserialize_state(nc_chain* chain, const void* data, size_t length) {
+    NC_ABI_BEGIN
+    NC_ARG(chain != nullptr, "null chain");
+    std::unique_ptr<NutcrackerState> st(Nutcracker_State_deserialize((uint32_t)length, data));
+    if (!st) throw nc::Error(nc::NC_ERR_ARG, Nutcracker_getError() ? Nutcracker_getError() : "bad state buffer");
+    std::vector<uint32_t> bonds{1};
+    std::vector<const nc_complex*> sites;
+    for (const SitePtr& s : st->sites) {
+        NC_ARG(s->cl == bonds.back(), "state site dimensions do not match");
+        bonds.push_back(s->cr);
+        sites.push_back(s->W.data());
+    }
+    nc_chain_info info;
+    if (nc_chain_get_info(chain, &info) != 0) throw nc::Error(nc_last_status(), nc_last_error());
+    NC_ARG(sites.size() == info.number_of_sites, "the state has a different number of sites than the chain");
+    for (uint32_t i = 0; i < info.number_of_sites; ++i) {
+        uint32_t dims[3];
+        if (nc_chain_get_site(chain, i, nullptr, dims) != 0) throw nc::Error(nc_last_status(), nc_last_error());
+        NC_ARG(dims[2] == st->sites[i]->d, "the state's physical dimensions differ from the chain's");
+    }
+    if (nc_chain_set_state(chain, bonds.data(), sites.data()) != 0) throw nc::Error(nc_last_status(), nc_last_error());
+    NC_ABI_END
+    return nc::g_status;
+}
+
+}  // extern "C"

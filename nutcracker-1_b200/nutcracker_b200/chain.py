@@ -79,6 +79,9 @@ lib.nc_chain_move_to.argtypes = [ct.c_void_p, ct.c_uint32]
 lib.nc_chain_set_precision.argtypes = [ct.c_void_p, ct.c_uint32]
 lib.nc_chain_solve_for_eigenvalues.argtypes = [ct.c_void_p, ct.c_uint32, ct.POINTER(ct.c_double)]
 lib.nc_chain_solve_levels_at_bandwidth.argtypes = [ct.c_void_p, ct.c_uint32, ct.POINTER(ct.c_double)]
+lib.nc_chain_serialize_state.restype = ct.c_size_t
+lib.nc_chain_serialize_state.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_size_t]
+lib.nc_chain_deserialize_state.argtypes = [ct.c_void_p, ct.c_char_p, ct.c_size_t]
 SIGNAL_FN = ct.CFUNCTYPE(None, ct.c_void_p, ct.c_int, ct.c_int64, ct.c_void_p)
 lib.nc_chain_connect.restype = ct.c_int64
 lib.nc_chain_connect.argtypes = [ct.c_void_p, ct.c_int, SIGNAL_FN, ct.c_void_p]
@@ -151,6 +154,19 @@ class Chain:
         if st != 0:
             _check()
             raise NutcrackerError(st, "chain call failed")
+
+    # -- checkpoint / resume (StateBuffer layout of nutcracker.proto) -----------
+    def serialize_state(self):
+        n = lib.nc_chain_serialize_state(self._h, None, 0)
+        if n == 0:
+            _check()
+        buf = ct.create_string_buffer(n)
+        if lib.nc_chain_serialize_state(self._h, buf, n) != n:
+            _check()
+        return buf.raw
+
+    def deserialize_state(self, data):
+        self._call(lib.nc_chain_deserialize_state, data, len(data))
 
     # -- signals (base_chain.hpp:54-60, chain.hpp:151) ------------------------
     def connect(self, signal, callback):

@@ -49,3 +49,23 @@ def test_disconnect_stops_callbacks():
     from nutcracker_b200 import NutcrackerError
     with pytest.raises(NutcrackerError):
         ch.disconnect(cid)
+
+
+def test_checkpoint_and_resume_a_converged_level():
+    """A converged state saved in the StateBuffer layout and loaded into a new
+    chain gives the same energy, and the C API reads the same bytes as a state."""
+    from nutcracker_b200 import capi
+    from nutcracker_b200.chain import Chain
+    ops = mpo.transverse_ising_ferro(8, 0.9)
+    a = Chain(ops, initial_bandwidth_dimension=16, seed=3)
+    a.sweep_until_converged()
+    e = a.get_energy()
+    data = a.serialize_state()
+    b = Chain(ops, initial_bandwidth_dimension=2, seed=11)
+    b.deserialize_state(data)
+    assert abs(b.compute_expectation_value() - e) < 1e-10 * abs(e)
+    assert abs(b.get_energy() - e) < 1e-10 * abs(e)
+    st = capi.State.deserialize(data)
+    assert abs(st.overlap(st) - 1) < 1e-10
+    again = capi.State.deserialize(b.serialize_state())
+    assert abs(abs(again.overlap(st)) - 1) < 1e-10
