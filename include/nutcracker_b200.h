@@ -192,6 +192,24 @@ void form_overlap_site_tensor_(const uint32_t* br, const uint32_t* bl, const uin
                                const nc_complex* state_site_tensor,
                                nc_complex* overlap_site_tensor);
 
+/* core.cpp:210-231 (contract_matrix_left_): L' (br,br) = M L M^H. */
+void contract_matrix_left_(const uint32_t* bl, const uint32_t* br, const nc_complex* left_environment,
+                           const nc_complex* matrix, nc_complex* new_left_environment);
+/* core.cpp:400-427 (extend_state_vector_fragment_, used by flat.cpp):
+   new (br,dr,dl) = sum_m site(br,m,dr) old(m,dl). */
+void extend_state_vector_fragment_(const uint32_t* bm, const uint32_t* br, const uint32_t* dl,
+                                   const uint32_t* dr, const nc_complex* old_state_vector_fragment,
+                                   const nc_complex* site_tensor, nc_complex* new_state_vector_fragment);
+/* core.cpp:785-818 (increase_bandwidth_with_environment_): the infinite-chain
+   routine; exported so the reference's C++ layer links, and always fails with
+   NC_ERR_ARG (the infinite chain is not supported). */
+void increase_bandwidth_with_environment_(const uint32_t* b, const uint32_t* c, const uint32_t* d,
+                                          const uint32_t* new_b, const nc_complex* old_state_site_tensor,
+                                          const nc_complex* old_left_exp_environment,
+                                          const nc_complex* old_right_exp_environment,
+                                          nc_complex* new_state_site_tensor, nc_complex* new_left_exp_environment,
+                                          nc_complex* new_right_exp_environment);
+
 /* ---- Level 0: site eigen-solve and projectors (core.cpp:109-441, 676-774) -------- */
 
 /* core.cpp:676-693 (optimize_): the site eigen-solve.  Returns the

@@ -416,4 +416,54 @@ void form_overlap_site_tensor_(const uint32_t* br, const uint32_t* bl, const uin
     NC_ABI_END
 }
 
+// core.f95:1195-1234 (contract_matrix_left): L' (br,br) = M L M^H for
+// M (br,bl), L (bl,bl).
+void contract_matrix_left_(const uint32_t* bl, const uint32_t* br, const nc_complex* left_environment,
+                           const nc_complex* matrix, nc_complex* new_left_environment) {
+    NC_ABI_BEGIN
+    HostStage h;
+    const int l = (int)*bl, r = (int)*br;
+    const cplx* dL = h.in(left_environment, (size_t)l * l);
+    const cplx* dM = h.in(matrix, (size_t)r * l);
+    cplx* T = h.out((size_t)r * l);
+    cplx* o = h.out((size_t)r * r);
+    zgemm(zgemm_params(OP_N, OP_N, r, l, l, dM, r, dL, l, T, r), h.ctx);
+    zgemm(zgemm_params(OP_N, OP_C, r, r, l, T, r, dM, r, o, r), h.ctx);
+    h.back(new_left_environment, o, (size_t)r * r);
+    h.sync();
+    NC_ABI_END
+}
+
+// core.f95:1163-1193 (extend_state_vector_fragment): new (br,dr,dl) =
+// site (br,bm,dr) permuted to (br,dr,bm) times old (bm,dl).
+void extend_state_vector_fragment_(const uint32_t* bm, const uint32_t* br, const uint32_t* dl, const uint32_t* dr,
+                                   const nc_complex* old_state_vector_fragment, const nc_complex* site_tensor,
+                                   nc_complex* new_state_vector_fragment) {
+    NC_ABI_BEGIN
+    HostStage h;
+    const int m = (int)*bm, r = (int)*br, a = (int)*dl, b = (int)*dr;
+    const cplx* dOld = h.in(old_state_vector_fragment, (size_t)m * a);
+    const cplx* dS = h.in(site_tensor, (size_t)r * m * b);
+    cplx* T = h.out((size_t)r * b * m);
+    cplx* o = h.out((size_t)r * b * a);
+    const int p_rs[3] = {0, 2, 1};
+    permute3(h.ctx, dS, r, m, b, p_rs, false, T);
+    zgemm(zgemm_params(OP_N, OP_N, r * b, a, m, T, r * b, dOld, m, o, r * b), h.ctx);
+    h.back(new_state_vector_fragment, o, (size_t)r * b * a);
+    h.sync();
+    NC_ABI_END
+}
+
+// core.f95:3246-3297 (increase_bandwidth_with_environment) belongs to the
+// infinite-chain path, which this library does not implement: the symbol is
+// exported so that a build of the reference's C++ layer links, and a call
+// reports NC_ERR_ARG through nc_last_status() and leaves its outputs untouched.
+void increase_bandwidth_with_environment_(const uint32_t*, const uint32_t*, const uint32_t*, const uint32_t*,
+                                          const nc_complex*, const nc_complex*, const nc_complex*, nc_complex*,
+                                          nc_complex*, nc_complex*) {
+    NC_ABI_BEGIN
+    throw nc::Error(nc::NC_ERR_ARG, "increase_bandwidth_with_environment_: the infinite chain is not supported");
+    NC_ABI_END
+}
+
 }  // extern "C"

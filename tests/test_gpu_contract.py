@@ -124,3 +124,32 @@ def test_bad_operator_index_reports_error(nb):
     W = np.ones((1, 1, 1), complex, order="F")
     with pytest.raises(nb.NutcrackerError):
         nb.Core.contract_sos_left(1, 1, 1, 1, 1, one, 1, idx, W, one)
+
+
+def test_contract_matrix_left_and_extend_state_vector_fragment():
+    """core.f95:1163-1234 restated in numpy: L' = M L M^H and the state-vector
+    fragment extension of flat.cpp."""
+    import ctypes as ct
+
+    import nutcracker_b200 as nb
+    from gpu_util import rand_c, rel_err
+
+    u = lambda x: ct.byref(ct.c_uint32(x))
+    p = lambda a: a.ctypes.data_as(ct.c_void_p)
+    rng = np.random.default_rng(17)
+    bl, br = 7, 5
+    L, M = rand_c(rng, (bl, bl)), rand_c(rng, (br, bl))
+    out = np.zeros((br, br), dtype=complex, order="F")
+    nb.lib.contract_matrix_left_(u(bl), u(br), p(L), p(M), p(out))
+    assert nb.lib.nc_last_status() == 0
+    assert rel_err(out, M @ L @ M.conj().T) < 1e-13
+    bm, br, dl, dr = 6, 4, 3, 2
+    old, S = rand_c(rng, (bm, dl)), rand_c(rng, (br, bm, dr))
+    new = np.zeros((br, dr, dl), dtype=complex, order="F")
+    nb.lib.extend_state_vector_fragment_(u(bm), u(br), u(dl), u(dr), p(old), p(S), p(new))
+    assert nb.lib.nc_last_status() == 0
+    assert rel_err(new, np.einsum("rms,ma->rsa", S, old)) < 1e-13
+    # the infinite-chain routine is exported but reports that it is unsupported
+    z = np.zeros(8, dtype=complex)
+    nb.lib.increase_bandwidth_with_environment_(u(1), u(1), u(2), u(2), p(z), p(z), p(z), p(z), p(z), p(z))
+    assert nb.lib.nc_last_status() != 0
