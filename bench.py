@@ -537,6 +537,28 @@ def run_reference(args, rank):
 # GPU arm
 # ---------------------------------------------------------------------------
 
+def max_over_ranks(x, dist, device):
+    """The largest of the ranks' values (times are reported as the slowest rank's)."""
+    if not dist:
+        return x
+    import torch
+    import torch.distributed as td
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    td.all_reduce(t, op=td.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_seed(seed, rank):
+    """Each replica sweeps its own chain from its own random initial state."""
+    return seed + 7919 * rank
+
+
+def replica_throughput(steps, world, seconds_max):
+    """Whole-job sweeps/s of `world` independent replicas that each time `steps`
+    sweeps: every rank's sweeps over the slowest rank's time."""
+    return steps * world / seconds_max
+
+
 def run_ours(args, rank, world):
     import ctypes as ct
     import torch
@@ -559,12 +581,6 @@ def run_ours(args, rank, world):
         if dist:
             td.barrier()
 
-    def max_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        td.all_reduce(t, op=td.ReduceOp.MAX)
-        return float(t.item())
 
     def timed_sweeps(chain, steps):
         barrier()
@@ -579,7 +595,7 @@ def run_ours(args, rank, world):
         torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         barrier()
-        return max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+        return max_over_ranks(ev0.elapsed_time(ev1) / 1e3, dist, "cuda")
 
     def query(kind):
         n, ms, fl = ct.c_uint64(), ct.c_double(), ct.c_double()
@@ -591,7 +607,7 @@ def run_ours(args, rank, world):
         nb.lib.nc_profile_end(ct.byref(n), ct.byref(ms), ct.byref(fl))
 
     ops = operators.heisenberg(args.sites)
-    chain = Chain(ops, initial_bandwidth_dimension=args.chi_start, seed=args.seed + 7919 * rank,
+    chain = Chain(ops, initial_bandwidth_dimension=args.chi_start, seed=replica_seed(args.seed, rank),
                   time_phases=1 if args.phases else 0)
     for _ in range(args.presweeps):
         chain.perform_optimization_sweep()
@@ -669,8 +685,8 @@ def run_ours(args, rank, world):
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
-        te = max_over_ranks(e0.elapsed_time(e1) / 1e3)
-        e2e = {"value": args.steps * world / te, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+        te = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist, "cuda")
+        e2e = {"value": replica_throughput(args.steps, world, te), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": 8, "precision": head, "wall_s": time.perf_counter() - t0}
 
     # FP64 GEMM peak measured live (MEASURED_PEAKS.json has no FP64 entry)
@@ -717,7 +733,7 @@ def run_ours(args, rank, world):
             "e2e": e2e, "clocks": clk}
     if "fp64" in res:
         r = res["fp64"]
-        v64 = args.steps * world / r["seconds"]
+        v64 = replica_throughput(args.steps, world, r["seconds"])
         ms, fl = r["gemm"][1], r["gemm"][2]
         ach = fl / ms / 1e12 if ms > 0 else None
         line["fp64"] = {"value": v64, "ms_per_step": r["seconds"] / args.steps * 1e3,
@@ -729,7 +745,7 @@ def run_ours(args, rank, world):
                                      "gemm_share_of_step": ms / r["seconds"]}}
     if "mixed" in res:
         r = res["mixed"]
-        vmx = args.steps * world / r["seconds"]
+        vmx = replica_throughput(args.steps, world, r["seconds"])
         ms, fl = r["tc"][1], r["tc"][2]
         ach = fl / ms / 1e12 if ms > 0 else None
         line.update({"value": vmx, "ms_per_step": r["seconds"] / args.steps * 1e3, "dtype": "3xTF32/f64",
