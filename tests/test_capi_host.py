@@ -230,3 +230,43 @@ def _len(b):
         out += bytes([(n & 0x7F) | 0x80])
         n >>= 7
     return out + bytes([n])
+
+
+def _enc(n):
+    out = b""
+    while n >= 0x80:
+        out += bytes([(n & 0x7F) | 0x80])
+        n >>= 7
+    return out + bytes([n])
+
+
+def _state_buffer(sites, norms=True):
+    """StateBuffer (nutcracker.proto) from (d, bl, br, complex array) sites."""
+    out = b""
+    for k, (d, bl, br, A) in enumerate(sites):
+        m = b""
+        if norms:
+            m += b"\x08" + _enc(0 if k == 0 else 2)
+        m += b"\x10" + _enc(d) + b"\x18" + _enc(bl) + b"\x20" + _enc(br)
+        raw = np.asarray(A, dtype=complex).ravel(order="F").view(np.float64).tobytes()
+        m += b"\x2a" + _enc(len(raw)) + raw
+        out += b"\x0a" + _enc(len(m)) + m
+    return out
+
+
+def test_state_buffer_round_trip_and_errors(C):
+    from nutcracker_b200 import NutcrackerError
+    rng = np.random.default_rng(4)
+    sites = [(2, 1, 3, rng.normal(size=(3, 1, 2)) + 1j * rng.normal(size=(3, 1, 2))),
+             (2, 3, 1, rng.normal(size=(1, 3, 2)))]
+    data = _state_buffer(sites)
+    assert C.State.deserialize(data).serialize() == data
+    # fields of an unknown number are skipped, a missing normalisation is accepted
+    st = C.State.deserialize(b"\x9a\x01\x02hi" + _state_buffer(sites, norms=False))
+    assert st.serialize() == data
+    with pytest.raises(NutcrackerError, match="does not match its dimensions"):
+        C.State.deserialize(_state_buffer([(2, 1, 3, np.zeros((3, 1, 1)))]))
+    with pytest.raises(NutcrackerError, match="state site dimensions do not match"):
+        C.State.deserialize(_state_buffer([sites[0], (2, 2, 1, np.zeros((1, 2, 2)))]))
+    with pytest.raises(NutcrackerError, match="at least one site"):
+        C.State.deserialize(b"")
