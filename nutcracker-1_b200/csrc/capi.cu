@@ -1056,7 +1056,8 @@ namespace {
 
 // State(CopyFrom<sites>) (states.hpp:473-488): the last site scaled to unit
 // norm, then the orthogonality centre moved to the first site, each site
-// passed becoming right-normalised (norm_denorm_going_left_).
+// passed becoming right-normalised (norm_denorm_going_left_) and each new
+// centre renormalised (states.cpp:94-164), so the state has unit norm.
 std::vector<SitePtr> canonical_state(const std::vector<SitePtr>& sites) {
     if (sites.empty()) throw std::runtime_error("a state needs at least one site");
     SiteData current = *sites.back();
@@ -1078,6 +1079,14 @@ std::vector<SitePtr> canonical_state(const std::vector<SitePtr>& sites) {
                                     normB.W.data()) != 0)
             library_error();
         rest.push_back(std::make_shared<SiteData>(normB));
+        // the new centre is renormalised, as the reference's cursor moves do
+        double n2 = 0;
+        for (const nc_complex& z : denA.W) n2 += z.re * z.re + z.im * z.im;
+        const double inv = n2 > 0 ? 1.0 / std::sqrt(n2) : 1.0;
+        for (nc_complex& z : denA.W) {
+            z.re *= inv;
+            z.im *= inv;
+        }
         current = denA;
     }
     std::vector<SitePtr> out{std::make_shared<SiteData>(current)};

@@ -235,7 +235,9 @@ __global__ void __launch_bounds__(PT) panel_apply_kernel(int mp, int jb, const c
 constexpr int BT_T = 1024;
 constexpr size_t BT_SMEM = sizeof(cplx) * ((size_t)2 * NB * (NB + 1) + NB * NB / 2);
 
-__global__ void __launch_bounds__(BT_T) build_t_kernel(int nb, const cplx* __restrict__ G,
+// G is either a matrix (ld nb) or, with nparts > 0, the sum of nparts NB x NB
+// partial Gram blocks (ld NB, stride NB*NB) added in index order.
+__global__ void __launch_bounds__(BT_T) build_t_kernel(int nb, const cplx* __restrict__ G, int nparts,
                                                       const cplx* __restrict__ tau, cplx* __restrict__ T,
                                                       int ldt) {
     extern __shared__ __align__(16) unsigned char bt_smem[];
@@ -245,7 +247,26 @@ __global__ void __launch_bounds__(BT_T) build_t_kernel(int nb, const cplx* __res
     const int tid = threadIdx.x;
     for (int e = tid; e < NB * NB; e += BT_T) {
         const int i = e % NB, j = e / NB;
-        Gs[i * (NB + 1) + j] = (i < j && j < nb) ? G[i + (long long)nb * j] : cmake(0, 0);
+        cplx g = cmake(0, 0);
+        if (i < j && j < nb) {
+            if (nparts > 0) {
+                double r0 = 0, i0 = 0, r1 = 0, i1 = 0;   // two interleaved chains, fixed order
+                int c = 0;
+                for (; c + 1 < nparts; c += 2) {
+                    const cplx a = G[(size_t)c * NB * NB + i + NB * j];
+                    const cplx b = G[(size_t)(c + 1) * NB * NB + i + NB * j];
+                    r0 += a.x; i0 += a.y; r1 += b.x; i1 += b.y;
+                }
+                if (c < nparts) {
+                    const cplx a = G[(size_t)c * NB * NB + i + NB * j];
+                    r0 += a.x; i0 += a.y;
+                }
+                g = cmake(r0 + r1, i0 + i1);
+            } else {
+                g = G[i + (long long)nb * j];
+            }
+        }
+        Gs[i * (NB + 1) + j] = g;
         Ts[i * (NB + 1) + j] = (i == j && i < nb) ? tau[i] : cmake(0, 0);
     }
     __syncthreads();
@@ -282,15 +303,170 @@ __global__ void __launch_bounds__(BT_T) build_t_kernel(int nb, const cplx* __res
     }
 }
 
-void launch_build_t(Context& ctx, int nb, const cplx* G, const cplx* tau, cplx* T) {
+void launch_build_t(Context& ctx, int nb, const cplx* G, const cplx* tau, cplx* T, int nparts = 0) {
     static bool attr = false;
     if (!attr) {
         NC_CUDA(cudaFuncSetAttribute(build_t_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BT_SMEM));
         attr = true;
     }
-    build_t_kernel<<<1, BT_T, BT_SMEM, ctx.stream>>>(nb, G, tau, T, NB);
+    build_t_kernel<<<1, BT_T, BT_SMEM, ctx.stream>>>(nb, G, nparts, tau, T, NB);
     NC_CHECK_LAUNCH();
     ctx.launches++;
+}
+
+// ---------------------------------------------------------------------------
+// One block reflector applied to one block of at most NB columns,
+//   C <- (I - V T V^H)^H C = C - V T^H (V^H C)     (V mp x nb, C mp x nc),
+// and the Gram matrix V^H V of the block, for the critical path of the
+// look-ahead QR.  The products are small (64 x 64 outputs, K = mp <= 2048),
+// so instead of split-K GEMMs on a handful of tiles they run as
+//   refl_partial_kernel: per 32-row chunk, the 64 x 64 partial of V^H C
+//                        (one CTA per chunk, operands staged in shared memory);
+//   refl_w2_kernel:      per column k, the chunk partials summed in chunk order
+//                        and W2(:,k) = T^H W(:,k);
+//   refl_apply_kernel:   per 32-row chunk, C -= V W2.
+// The Gram matrix is refl_partial_kernel with C = V, its partials summed by
+// build_t_kernel.  Every sum runs in a fixed order (bit-reproducible).
+// ---------------------------------------------------------------------------
+constexpr int RC = 32;                                     // rows per chunk
+constexpr int RT = 256;                                    // threads
+constexpr int RL = NB + 1;                                 // padded shared-memory row
+constexpr size_t RP_SMEM = sizeof(cplx) * 2 * RC * RL;     // V and C chunks
+constexpr size_t RA_SMEM = sizeof(cplx) * (NB + RC) * RL;  // W2 and the V chunk
+
+__global__ void __launch_bounds__(RT) refl_partial_kernel(int mp, int nb, const cplx* __restrict__ V, long long ldv,
+                                                          const cplx* __restrict__ C, long long ldc, int nc,
+                                                          cplx* __restrict__ part) {
+    extern __shared__ __align__(16) unsigned char rp_smem[];
+    cplx* Vs = reinterpret_cast<cplx*>(rp_smem);   // [RC][RL]
+    cplx* Cs = Vs + RC * RL;                         // [RC][RL]
+    const int r0 = blockIdx.x * RC, tid = threadIdx.x;
+    for (int e = tid; e < RC * NB; e += RT) {
+        const int r = e % RC, c = e / RC, row = r0 + r;
+        Vs[r * RL + c] = (row < mp && c < nb) ? V[row + ldv * c] : cmake(0, 0);
+        Cs[r * RL + c] = (row < mp && c < nc) ? C[row + ldc * c] : cmake(0, 0);
+    }
+    __syncthreads();
+    const int k = tid % NB, i0 = (tid / NB) * (NB / 4);   // 16 outputs (i0..i0+15, k) per thread
+    double ar[NB / 4], ai[NB / 4];
+#pragma unroll
+    for (int q = 0; q < NB / 4; ++q) ar[q] = ai[q] = 0;
+    for (int r = 0; r < RC; ++r) {
+        const cplx c = Cs[r * RL + k];
+#pragma unroll
+        for (int q = 0; q < NB / 4; ++q) {
+            const cplx v = Vs[r * RL + i0 + q];   // conj(v) * c
+            ar[q] = fma(v.x, c.x, fma(v.y, c.y, ar[q]));
+            ai[q] = fma(v.x, c.y, fma(-v.y, c.x, ai[q]));
+        }
+    }
+    cplx* out = part + (size_t)blockIdx.x * NB * NB;
+#pragma unroll
+    for (int q = 0; q < NB / 4; ++q) out[i0 + q + NB * k] = cmake(ar[q], ai[q]);
+}
+
+__global__ void __launch_bounds__(RT) refl_w2_kernel(int nparts, int nb, const cplx* __restrict__ part,
+                                                     const cplx* __restrict__ T, int ldt, cplx* __restrict__ W2) {
+    __shared__ cplx red[RT / NB][NB];
+    __shared__ cplx Ws[NB];
+    const int k = blockIdx.x, tid = threadIdx.x, i = tid % NB, q = tid / NB;
+    double sr = 0, si = 0;
+    for (int c = q; c < nparts; c += RT / NB) {
+        const cplx a = part[(size_t)c * NB * NB + i + NB * k];
+        sr += a.x;
+        si += a.y;
+    }
+    red[q][i] = cmake(sr, si);
+    __syncthreads();
+    if (q == 0) {
+        cplx w = red[0][i];
+#pragma unroll
+        for (int g = 1; g < RT / NB; ++g) w = cadd(w, red[g][i]);
+        Ws[i] = w;
+    }
+    __syncthreads();
+    if (q == 0) {
+        // W2(i,k) = sum_{l <= i} conj(T(l,i)) W(l,k)   (T upper triangular)
+        double wr = 0, wi = 0;
+        if (i < nb)
+            for (int l = 0; l <= i; ++l) {
+                const cplx t = T[l + (long long)ldt * i], w = Ws[l];
+                wr = fma(t.x, w.x, fma(t.y, w.y, wr));
+                wi = fma(t.x, w.y, fma(-t.y, w.x, wi));
+            }
+        W2[i + NB * k] = cmake(wr, wi);
+    }
+}
+
+__global__ void __launch_bounds__(RT) refl_apply_kernel(int mp, int nb, const cplx* __restrict__ V, long long ldv,
+                                                        const cplx* __restrict__ W2, cplx* __restrict__ C,
+                                                        long long ldc, int nc) {
+    extern __shared__ __align__(16) unsigned char ra_smem[];
+    cplx* Ws = reinterpret_cast<cplx*>(ra_smem);   // [NB][RL]: Ws[l * RL + k] = W2(l,k)
+    cplx* Vs = Ws + NB * RL;                         // [RC][RL]
+    const int r0 = blockIdx.x * RC, tid = threadIdx.x;
+    for (int e = tid; e < NB * NB; e += RT) {
+        const int l = e % NB, kk = e / NB;
+        Ws[l * RL + kk] = (l < nb && kk < nc) ? W2[l + NB * kk] : cmake(0, 0);
+    }
+    for (int e = tid; e < RC * NB; e += RT) {
+        const int r = e % RC, c = e / RC, row = r0 + r;
+        Vs[r * RL + c] = (row < mp && c < nb) ? V[row + ldv * c] : cmake(0, 0);
+    }
+    __syncthreads();
+    const int k = tid % NB, rq = (tid / NB) * (RC / 4);   // rows rq..rq+7 of column k
+    if (k >= nc) return;
+    double ar[RC / 4], ai[RC / 4];
+#pragma unroll
+    for (int q = 0; q < RC / 4; ++q) ar[q] = ai[q] = 0;
+    for (int l = 0; l < NB; ++l) {
+        const cplx w = Ws[l * RL + k];
+#pragma unroll
+        for (int q = 0; q < RC / 4; ++q) {
+            const cplx v = Vs[(rq + q) * RL + l];
+            ar[q] = fma(v.x, w.x, fma(-v.y, w.y, ar[q]));
+            ai[q] = fma(v.x, w.y, fma(v.y, w.x, ai[q]));
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < RC / 4; ++q) {
+        const int row = r0 + rq + q;
+        if (row < mp) {
+            cplx& c = C[row + ldc * k];
+            c = cmake(c.x - ar[q], c.y - ai[q]);
+        }
+    }
+}
+
+int refl_chunks(int mp) { return (mp + RC - 1) / RC; }
+
+void refl_attrs() {
+    static bool attr = false;
+    if (!attr) {
+        NC_CUDA(cudaFuncSetAttribute(refl_partial_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RP_SMEM));
+        NC_CUDA(cudaFuncSetAttribute(refl_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RA_SMEM));
+        attr = true;
+    }
+}
+
+// part (refl_chunks(mp) x NB x NB) = chunk partials of V^H C.
+void launch_refl_partial(Context& ctx, int mp, int nb, const cplx* V, long long ldv, const cplx* C, long long ldc,
+                         int nc, cplx* part) {
+    refl_attrs();
+    refl_partial_kernel<<<refl_chunks(mp), RT, RP_SMEM, ctx.stream>>>(mp, nb, V, ldv, C, ldc, nc, part);
+    NC_CHECK_LAUNCH();
+    ctx.launches++;
+}
+
+// C -= V T^H (V^H C), from the chunk partials of V^H C.
+void launch_refl_finish(Context& ctx, int mp, int nb, const cplx* V, long long ldv, const cplx* T, int ldt,
+                        const cplx* part, cplx* W2, cplx* C, long long ldc, int nc) {
+    refl_attrs();
+    refl_w2_kernel<<<nc, RT, 0, ctx.stream>>>(refl_chunks(mp), nb, part, T, ldt, W2);
+    NC_CHECK_LAUNCH();
+    refl_apply_kernel<<<refl_chunks(mp), RT, RA_SMEM, ctx.stream>>>(mp, nb, V, ldv, W2, C, ldc, nc);
+    NC_CHECK_LAUNCH();
+    ctx.launches += 2;
 }
 
 // ---------------------------------------------------------------------------
@@ -660,8 +836,8 @@ void householder_qr_lookahead(Context& ctx, Context& side, cudaEvent_t* ev, int 
     cplx* V = ar.alloc_n<cplx>((size_t)m * n);
     cplx* tau = ar.alloc_n<cplx>(n);
     cplx* Tb = ar.alloc_n<cplx>((size_t)nblocks * NB * NB);
-    cplx* G = ar.alloc_n<cplx>(NB * NB);
-    cplx* Wm = ar.alloc_n<cplx>(NB * NB);
+    cplx* Gpart = ar.alloc_n<cplx>((size_t)refl_chunks(m) * NB * NB);
+    cplx* Wpart = ar.alloc_n<cplx>((size_t)refl_chunks(m) * NB * NB);
     cplx* W2m = ar.alloc_n<cplx>(NB * NB);
     cplx* Ws = ar.alloc_n<cplx>((size_t)NB * n);
     cplx* W2s = ar.alloc_n<cplx>((size_t)NB * n);
@@ -680,10 +856,10 @@ void householder_qr_lookahead(Context& ctx, Context& side, cudaEvent_t* ev, int 
         const cplx* Vb = V + j0 + j0 * (long long)m;
         cplx* T = Tb + (size_t)ob * NB * NB;
         cudaEvent_t ev_t = ev[2 + 2 * ob], ev_bulk = ev[3 + 2 * ob];
-        // main: factor block ob, then T_ob
+        // main: factor block ob, then T_ob from the chunk partials of V^H V
         launch_cluster_block(ctx, mp, nb, A + j0 + j0 * lda, lda, V + j0 + j0 * (long long)m, m, tau + j0);
-        zgemm(zgemm_params(OP_C, OP_N, nb, nb, mp, Vb, m, Vb, m, G, nb), ctx);
-        launch_build_t(ctx, nb, G, tau + j0, T);
+        launch_refl_partial(ctx, mp, nb, Vb, m, Vb, m, nb, Gpart);
+        launch_build_t(ctx, nb, Gpart, tau + j0, T, refl_chunks(mp));
         NC_CUDA(cudaEventRecord(ev_t, ctx.stream));
         const int j1 = j0 + nb, nb1 = (ob + 1 < nblocks) ? std::min(NB, n - j1) : 0;
         if (nb1 > 0) {
@@ -691,12 +867,8 @@ void householder_qr_lookahead(Context& ctx, Context& side, cudaEvent_t* ev, int 
             // those columns by reflector ob-1
             if (ob > 0) NC_CUDA(cudaStreamWaitEvent(ctx.stream, ev[3 + 2 * (ob - 1)], 0));
             cplx* A1 = A + j0 + j1 * lda;
-            zgemm(zgemm_params(OP_C, OP_N, nb, nb1, mp, Vb, m, A1, lda, Wm, nb), ctx);
-            zgemm(zgemm_params(OP_C, OP_N, nb, nb1, nb, T, NB, Wm, nb, W2m, nb), ctx);
-            ZGemmParams p = zgemm_params(OP_N, OP_N, mp, nb1, nb, Vb, m, W2m, nb, A1, lda);
-            p.alpha = cmake(-1, 0);
-            p.beta = cmake(1, 0);
-            zgemm(p, ctx);
+            launch_refl_partial(ctx, mp, nb, Vb, m, A1, lda, nb1, Wpart);
+            launch_refl_finish(ctx, mp, nb, Vb, m, T, NB, Wpart, W2m, A1, lda, nb1);
         }
         // side: reflector ob on the columns after block ob+1, then Q
         NC_CUDA(cudaStreamWaitEvent(side.stream, ev_t, 0));

@@ -29,7 +29,7 @@ def test_piped_four_levels_match_reference_energies():
     assert set(conf) == {"site convergence tolerance", "sweep convergence tolerance",
                          "chain convergence tolerance", "sanity check threshold"}
     levels = out["Energy levels"]
-    assert len(levels) == 4
+    assert len(levels) == 4, r.stderr
     for e, ref in zip(levels, REF):
         assert abs(e - ref) <= 1e-9 * abs(ref), (levels, REF)
 
