@@ -22,7 +22,12 @@ def run(args, stdin=b"", cwd=None):
 
 
 def test_piped_four_levels_match_reference_energies():
-    r = run(["-n", "4"], stdin=open(TFIM, "rb").read())
+    # the options of the reference's four-level stress test (tests/stress.cpp:107-186:
+    # initial bond dimension 2, site 1e-10, sweep and chain 1e-9, sanity 1e-12),
+    # which pins these energies to 1e-7
+    r = run(["-n", "4", "--initial-bandwidth", "2", "--site-tolerance", "1e-10", "--sweep-tolerance", "1e-9",
+             "--chain-tolerance", "1e-9", "--sanity-tolerance", "1e-12", "--seed", "6"],
+            stdin=open(TFIM, "rb").read())
     assert r.returncode == 0, r.stderr
     out = yaml.safe_load(r.stdout)
     conf = out["Configuration"]
@@ -31,7 +36,7 @@ def test_piped_four_levels_match_reference_energies():
     levels = out["Energy levels"]
     assert len(levels) == 4, r.stderr
     for e, ref in zip(levels, REF):
-        assert abs(e - ref) <= 1e-9 * abs(ref), (levels, REF)
+        assert abs(e - ref) <= 1e-7 * abs(ref), (levels, REF)
 
 
 def test_file_input_location_output_file_and_overwrite(tmp_path):
