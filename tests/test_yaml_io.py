@@ -163,3 +163,15 @@ def test_malformed_yaml_is_rejected(yio):
                 "    matrices:\n      - {from: 1, to: 1, data: *nope}\nsequence: [1]\n"]:
         with pytest.raises(NutcrackerError):
             yio.read_operator(bad)
+
+
+def test_line_endings_quoted_keys_and_flow_documents(yio):
+    text = open(os.path.join(HERE, "golden", "yaml", "external_field_anchors_5.yaml")).read()
+    want = yio.read_operator(text)
+    for variant in (text.replace("\n", "\r\n"), text.replace("physical dimension", '"physical dimension"')):
+        got = yio.read_operator(variant)
+        assert all(np.array_equal(a.W, b.W) and np.array_equal(a.idx, b.idx) for a, b in zip(got, want))
+    flow = ("{sites: [{physical dimension: 2, left dimension: 1, right dimension: 1, "
+            "matrices: [{from: 1, to: 1, data: [1, 0, 0, -1]}]}], sequence: [1]}")
+    (s,) = yio.read_operator(flow)
+    assert np.array_equal(s.W[:, :, 0], np.diag([1, -1]))
