@@ -175,3 +175,16 @@ def test_line_endings_quoted_keys_and_flow_documents(yio):
             "matrices: [{from: 1, to: 1, data: [1, 0, 0, -1]}]}], sequence: [1]}")
     (s,) = yio.read_operator(flow)
     assert np.array_equal(s.W[:, :, 0], np.diag([1, -1]))
+
+
+@pytest.mark.parametrize("name", ["heisenberg", "spin1", "xxz"])
+def test_reader_reads_the_oracles_yaml(yio, name):
+    """Operators written by the oracle's own YAML emitter read back identically."""
+    from oracle import mpo
+    ops = {"heisenberg": lambda: mpo.heisenberg(7), "spin1": lambda: mpo.heisenberg_spin1(5, 0.5),
+           "xxz": lambda: mpo.xxz_random(6, np.random.default_rng(3))}[name]()
+    got = yio.read_operator(mpo.to_yaml(ops))
+    assert len(got) == len(ops)
+    for a, b in zip(got, ops):
+        assert (a.d, a.cl, a.cr) == (b.d, b.cl, b.cr)
+        assert np.array_equal(a.idx, b.idx) and np.allclose(a.W, b.W, rtol=0, atol=0)
