@@ -270,3 +270,49 @@ def test_state_buffer_round_trip_and_errors(C):
         C.State.deserialize(_state_buffer([sites[0], (2, 2, 1, np.zeros((1, 2, 2)))]))
     with pytest.raises(NutcrackerError, match="at least one site"):
         C.State.deserialize(b"")
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_random_term_sets_compile_to_their_hamiltonian(C, seed):
+    """Random sums of product, scaled local-field and neighbour-coupling terms on
+    sites of mixed dimension: the compiled operator equals the sum of the terms'
+    Kronecker products."""
+    rng = np.random.default_rng(100 + seed)
+    n = int(rng.integers(2, 5))
+    dims = [int(x) for x in rng.integers(2, 4, size=n)]
+
+    def rmat(d):
+        return rng.normal(size=(d, d)) + 1j * rng.normal(size=(d, d))
+
+    def kron_terms(terms):
+        H = 0
+        for t in terms:
+            P = np.eye(1)
+            for s in range(n):
+                P = np.kron(P, t.get(s, np.eye(dims[s])))
+            H = H + P
+        return H
+
+    b = C.OperatorBuilder(dims)
+    terms = []
+    for _ in range(int(rng.integers(1, 6))):
+        kind = int(rng.integers(0, 3))
+        if kind == 0:
+            comps = [rmat(d) for d in dims]
+            b.add_product_term([C.Matrix.new(m) for m in comps])
+            terms.append(dict(enumerate(comps)))
+        elif kind == 1:
+            s = int(rng.integers(0, n))
+            m = rmat(dims[s])
+            c = complex(rng.normal(), rng.normal())
+            b.add_term(c * C.OperatorTerm.local_external_field(s, C.Matrix.new(m)))
+            terms.append({s: c * m})
+        else:
+            s = int(rng.integers(0, n - 1))
+            ml, mr = rmat(dims[s]), rmat(dims[s + 1])
+            b.add_term(C.OperatorTerm.local_neighbor_coupling_field(s, C.Matrix.new(ml), C.Matrix.new(mr)))
+            terms.append({s: ml, s + 1: mr})
+    H, sites = dense(C, b.compile())
+    want = kron_terms(terms)
+    assert np.allclose(H, want, atol=1e-12 * max(1.0, np.abs(want).max()))
+    assert [s.d for s in sites] == dims
