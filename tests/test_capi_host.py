@@ -316,3 +316,17 @@ def test_random_term_sets_compile_to_their_hamiltonian(C, seed):
     want = kron_terms(terms)
     assert np.allclose(H, want, atol=1e-12 * max(1.0, np.abs(want).max()))
     assert [s.d for s in sites] == dims
+
+
+def test_heisenberg_from_bond_terms_compiles_to_bond_dimension_five(C):
+    """Sum over bonds of XX + YY + ZZ, added bond by bond: merging equivalent
+    signals leaves the minimal automaton (start, X, Y, Z, end)."""
+    n = 6
+    b = C.OperatorBuilder([2] * n)
+    for s in range(n - 1):
+        for p in "XYZ":
+            b.add_term(C.OperatorTerm.local_neighbor_coupling_field(s, C.Matrix.pauli(p), C.Matrix.pauli(p)))
+    H, sites = dense(C, b.compile())
+    want = kron_sum(n, [{s: P, s + 1: P} for s in range(n - 1) for P in (X, Y, Z)])
+    assert np.allclose(H, want, atol=1e-13)
+    assert [s.cr for s in sites] == [4] + [5] * (n - 3) + [4, 1]
