@@ -88,3 +88,13 @@ def test_configuration_file(tmp_path):
     (tmp_path / "other.cfg").write_text("bogus = 1\n")
     r = run(["-C", str(tmp_path / "other.cfg")], cwd=tmp_path)
     assert r.returncode == 255 and b"unrecognised option 'bogus' in the configuration file" in r.stderr
+
+
+def test_option_forms():
+    """--name=value and -nVALUE parse like the spaced forms; bad values are rejected."""
+    r = run(["--optimizer-mode=zz"])
+    assert r.returncode == 255 and b"There is no such optimizer mode 'zz'." in r.stderr
+    r = run(["-nx"])
+    assert r.returncode == 255 and b"the argument ('x') for option '--number-of-levels' is invalid" in r.stderr
+    r = run(["--number-of-levels", "-3"])
+    assert r.returncode == 255 and b"is invalid" in r.stderr
