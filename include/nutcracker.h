@@ -41,6 +41,10 @@ void Nutcracker_setError(char const* message);
 
 /* ---- square matrices (matrix.cpp); data row-major, dimension^2 entries ---- */
 void Nutcracker_Matrix_free(NutcrackerMatrix* matrix);
+/* includes/nutcracker.h:29-35: the Pauli matrices as exported constants,
+   owned by the library (the same objects the getters below return). */
+extern NutcrackerMatrix const *Nutcracker_Matrix_Pauli_I, *Nutcracker_Matrix_Pauli_X,
+    *Nutcracker_Matrix_Pauli_Y, *Nutcracker_Matrix_Pauli_Z;
 NutcrackerMatrix const* Nutcracker_Matrix_getPauliI(void);   /* owned by the library */
 NutcrackerMatrix const* Nutcracker_Matrix_getPauliX(void);
 NutcrackerMatrix const* Nutcracker_Matrix_getPauliY(void);
@@ -132,6 +136,9 @@ NutcrackerStateTerm* Nutcracker_StateTerm_create_W(NutcrackerVector const* commo
 
 /* ---- vectors (vector.cpp) ---- */
 void Nutcracker_Vector_free(NutcrackerVector* vector);
+/* includes/nutcracker.h:148-151: the qubit basis vectors up = (1, 0) and
+   down = (0, 1), owned by the library. */
+extern NutcrackerVector const *Nutcracker_Vector_Qubit_Up, *Nutcracker_Vector_Qubit_Down;
 NutcrackerVector* Nutcracker_Vector_new(uint32_t physical_dimension, NutcrackerComplex const* data);
 NutcrackerVector* Nutcracker_Vector_newBasis(uint32_t physical_dimension, uint32_t observed_value);
 NutcrackerVector* Nutcracker_Vector_add(NutcrackerVector const* x, NutcrackerVector const* y);

@@ -113,7 +113,10 @@ int nc_tc_zgemm_dev(uint32_t M, uint32_t N, uint32_t K, const void* A_dev, const
    device address up (cudaGetSymbolAddress); make it before any stream
    capture.  All calls share the array and each rewrites it completely, so
    nothing needs clearing, but calls that overlap on the GPU race: order them
-   on one stream.  Returns a status code. */
+   on one stream.  The (from, to) indices in idx_dev stay on the device and
+   are not range-checked: each pair must satisfy 1 <= from <= cl and
+   1 <= to <= cr.  Every dimension must be at least 1 (checked).
+   Returns a status code. */
 int nc_heff_apply_dev_noalloc(uint32_t bl, uint32_t br, uint32_t cl, uint32_t cr, uint32_t d,
                               uint32_t nnz, const uint32_t* idx_dev, const void* W_dev,
                               const void* L_dev, const void* R_dev, const void* x_dev,

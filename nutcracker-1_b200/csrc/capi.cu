@@ -801,6 +801,12 @@ NutcrackerMatrix const* Nutcracker_Matrix_getPauliX(void) { return pauli(1); }
 NutcrackerMatrix const* Nutcracker_Matrix_getPauliY(void) { return pauli(2); }
 NutcrackerMatrix const* Nutcracker_Matrix_getPauliZ(void) { return pauli(3); }
 
+// The exported constants of includes/nutcracker.h:29-35 (defined in the
+// reference's c-interface/matrix.cpp:8-11): the same library-owned objects
+// the getters return, set when the library is loaded.
+NutcrackerMatrix const *Nutcracker_Matrix_Pauli_I = pauli(0), *Nutcracker_Matrix_Pauli_X = pauli(1),
+                       *Nutcracker_Matrix_Pauli_Y = pauli(2), *Nutcracker_Matrix_Pauli_Z = pauli(3);
+
 NutcrackerMatrix* Nutcracker_Matrix_new(uint32_t dimension, NutcrackerComplex const* data) {
     C_BEGIN
     if (!data && dimension) throw std::invalid_argument("null matrix data");
@@ -837,6 +843,22 @@ void Nutcracker_Matrix_getElementAtCoordinate(NutcrackerMatrix const* x, uint32_
 
 // ---- vectors (vector.cpp) ----
 void Nutcracker_Vector_free(NutcrackerVector* vector) { delete vector; }
+
+// The qubit basis vectors up = (1, 0) and down = (0, 1) of
+// includes/nutcracker.h:148-151 (c-interface/vector.cpp:10-11,
+// utilities.cpp:120-121), owned by the library.
+static NutcrackerVector const* qubit(int which) {
+    static const NutcrackerVector* q[2] = {nullptr, nullptr};
+    static const bool init = [] {
+        const cd up[2] = {1, 0}, down[2] = {0, 1};
+        q[0] = new NutcrackerVector{make_vector(2, up)};
+        q[1] = new NutcrackerVector{make_vector(2, down)};
+        return true;
+    }();
+    (void)init;
+    return q[which];
+}
+NutcrackerVector const *Nutcracker_Vector_Qubit_Up = qubit(0), *Nutcracker_Vector_Qubit_Down = qubit(1);
 NutcrackerVector* Nutcracker_Vector_new(uint32_t physical_dimension, NutcrackerComplex const* data) {
     C_BEGIN
     if (!data && physical_dimension) throw std::invalid_argument("null vector data");

@@ -29,16 +29,16 @@ namespace {
 // the allocating thread's stream): freeing a chain never synchronises the
 // whole device, so chains run by other threads (the serving loop) keep going.
 void keep_pool_memory() {
-    static bool done = false;
-    if (done) return;
-    int dev = 0;
-    cudaMemPool_t pool;
-    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-        uint64_t keep = UINT64_MAX;   // freed blocks stay in this process's pool
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-    }
-    cudaGetLastError();
-    done = true;
+    static PerDeviceOnce once;   // the pool attribute belongs to each device's default pool
+    once([] {
+        int dev = 0;
+        cudaMemPool_t pool;
+        if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;   // freed blocks stay in this process's pool
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        cudaGetLastError();
+    });
 }
 
 struct DevBuf {

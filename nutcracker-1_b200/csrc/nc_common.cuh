@@ -8,6 +8,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <stdexcept>
@@ -120,5 +121,35 @@ struct Context {
 };
 
 inline unsigned ceil_div(size_t a, size_t b) { return (unsigned)((a + b - 1) / b); }
+
+// Runs a set-up step (a kernel attribute, which belongs to the device context
+// current when it is set) once per device.  One object per call site; safe
+// for concurrent callers (the step may run twice, so it must be idempotent).
+// Devices beyond the 64 tracked ones run the step on every call.
+class PerDeviceOnce {
+   public:
+    template <class F>
+    void operator()(F&& step) {
+        int dev = 0;
+        NC_CUDA(cudaGetDevice(&dev));
+        const uint64_t bit = (dev >= 0 && dev < 64) ? (1ull << dev) : 0ull;
+        if (bit && (done_.load(std::memory_order_acquire) & bit)) return;
+        step();
+        if (bit) done_.fetch_or(bit, std::memory_order_acq_rel);
+    }
+
+   private:
+    std::atomic<uint64_t> done_{0};
+};
+
+// The largest dynamic shared memory of `kernel`, set once per device.
+#define NC_SET_SMEM_ONCE(kernel, bytes)                                                             \
+    do {                                                                                            \
+        static ::nc::PerDeviceOnce _once;                                                           \
+        _once([&] {                                                                                 \
+            NC_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,       \
+                                         (int)(bytes)));                                            \
+        });                                                                                         \
+    } while (0)
 
 }  // namespace nc

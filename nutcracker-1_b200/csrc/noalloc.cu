@@ -20,6 +20,12 @@
 //   writes T and U completely before reading them.  Calls whose kernels
 //   overlap on the GPU (different streams, or different host threads on one
 //   device without ordering) race on the array; order them on one stream.
+// * The MPO indices live in device memory and are not read back (that would
+//   synchronise), so they are not range-checked: every (from, to) pair must
+//   satisfy 1 <= from <= cl and 1 <= to <= cr, or the mix kernel reads
+//   outside T.  The host-buffer entry points (optimize_ and friends) do
+//   check them.
+#include <climits>
 #include <mutex>
 
 #include "nc_abi_util.h"
@@ -60,13 +66,28 @@ extern "C" int nc_heff_apply_dev_noalloc(uint32_t bl, uint32_t br, uint32_t cl, 
                                          const void* L_dev, const void* R_dev, const void* x_dev, void* y_dev,
                                          void* stream) {
     NC_ABI_BEGIN
+    // Sizes are checked as unsigned 64-bit products before anything is cast
+    // to int, so no wrapped product can slip under the capacity check.
+    NC_ARG(bl >= 1 && br >= 1 && cl >= 1 && cr >= 1 && d >= 1 && nnz >= 1,
+           "nc_heff_apply_dev_noalloc: every dimension must be at least 1");
+    NC_ARG(bl <= INT_MAX && br <= INT_MAX && cl <= INT_MAX && cr <= INT_MAX && d <= INT_MAX && nnz <= INT_MAX,
+           "nc_heff_apply_dev_noalloc: dimension too large");
+    uint64_t need = 0;
+    {
+        uint64_t brbld = 0, elems = 0;
+        const bool wrap = __builtin_mul_overflow((uint64_t)br, (uint64_t)bl, &brbld) ||
+                          __builtin_mul_overflow(brbld, (uint64_t)d, &brbld) ||
+                          __builtin_mul_overflow(brbld, (uint64_t)cl + (uint64_t)cr, &elems) ||
+                          __builtin_mul_overflow(elems, (uint64_t)sizeof(cplx), &need);
+        if (wrap) need = UINT64_MAX;
+    }
+    if (need > kScratchBytes)
+        throw Error(NC_ERR_ARG, "nc_heff_apply_dev_noalloc: needs " +
+                                    (need == UINT64_MAX ? std::string("more than 2^64") : std::to_string(need)) +
+                                    " bytes of scratch, more than the fixed 67108864-byte (64 MiB) maximum");
     MpoSite op;
     op.d = (int)d; op.cl = (int)cl; op.cr = (int)cr; op.nnz = (int)nnz;
     op.idx = idx_dev; op.W = static_cast<const cplx*>(W_dev);
-    const size_t need = heff_workspace_elems((int)bl, (int)br, op) * sizeof(cplx);
-    if (need > kScratchBytes)
-        throw Error(NC_ERR_ARG, "nc_heff_apply_dev_noalloc: needs " + std::to_string(need) +
-                                    " bytes of scratch, more than the fixed 67108864-byte (64 MiB) maximum");
     cplx* ws = scratch_for_current_device();
     heff_apply_stream(static_cast<cudaStream_t>(stream), (int)bl, (int)br, op, static_cast<const cplx*>(L_dev),
                       static_cast<const cplx*>(R_dev), static_cast<const cplx*>(x_dev), static_cast<cplx*>(y_dev),

@@ -304,11 +304,7 @@ __global__ void __launch_bounds__(BT_T) build_t_kernel(int nb, const cplx* __res
 }
 
 void launch_build_t(Context& ctx, int nb, const cplx* G, const cplx* tau, cplx* T, int nparts = 0) {
-    static bool attr = false;
-    if (!attr) {
-        NC_CUDA(cudaFuncSetAttribute(build_t_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BT_SMEM));
-        attr = true;
-    }
+    NC_SET_SMEM_ONCE(build_t_kernel, BT_SMEM);
     build_t_kernel<<<1, BT_T, BT_SMEM, ctx.stream>>>(nb, G, nparts, tau, T, NB);
     NC_CHECK_LAUNCH();
     ctx.launches++;
@@ -441,12 +437,8 @@ __global__ void __launch_bounds__(RT) refl_apply_kernel(int mp, int nb, const cp
 int refl_chunks(int mp) { return (mp + RC - 1) / RC; }
 
 void refl_attrs() {
-    static bool attr = false;
-    if (!attr) {
-        NC_CUDA(cudaFuncSetAttribute(refl_partial_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RP_SMEM));
-        NC_CUDA(cudaFuncSetAttribute(refl_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RA_SMEM));
-        attr = true;
-    }
+    NC_SET_SMEM_ONCE(refl_partial_kernel, RP_SMEM);
+    NC_SET_SMEM_ONCE(refl_apply_kernel, RA_SMEM);
 }
 
 // part (refl_chunks(mp) x NB x NB) = chunk partials of V^H C.
@@ -651,10 +643,9 @@ cluster_block_qr_kernel(int mp, int nb, int rows_per_cta, cplx* __restrict__ A, 
 
 // Cluster launch support (size CQ_MAXC needs the non-portable opt-in); a
 // device that cannot co-schedule the cluster uses the per-panel path.
-bool cluster_qr_available() {
-    static int state = -1;
-    if (state >= 0) return state == 1;
-    state = 0;
+// The attribute and the answer belong to each device, so both are kept per
+// device (the first 64; others are probed on every call).
+bool cluster_qr_probe() {
     if (cudaFuncSetAttribute(cluster_block_qr_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
         cudaSuccess) {
         cudaGetLastError();
@@ -675,8 +666,20 @@ bool cluster_qr_available() {
         cudaGetLastError();
         return false;
     }
-    state = nclusters >= 1 ? 1 : 0;
-    return state == 1;
+    return nclusters >= 1;
+}
+
+bool cluster_qr_available() {
+    static std::atomic<int> state[64];   // 0 unknown, 1 available, 2 not available
+    int dev = 0;
+    NC_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return cluster_qr_probe();
+    int s = state[dev].load(std::memory_order_acquire);
+    if (s == 0) {
+        s = cluster_qr_probe() ? 1 : 2;
+        state[dev].store(s, std::memory_order_release);
+    }
+    return s == 1;
 }
 
 void launch_cluster_block(Context& ctx, int mp, int nb, cplx* A, long long lda, cplx* V, long long ldv,

@@ -329,11 +329,7 @@ CUtensorMap make_map(const float* ptr, int Kr, int rows, long long ld, long long
 void tc_gemm(Context& ctx, const TcGemm& g) {
     NC_ARG(g.M >= 1 && g.Nr >= 2 && g.Kr >= 1 && g.batch >= 1, "tc32: empty GEMM");
     NC_ARG(g.Nr % 2 == 0, "tc32: Nr must be even (complex columns)");
-    static bool attr = false;
-    if (!attr) {
-        NC_CUDA(cudaFuncSetAttribute(tc32_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
-        attr = true;
-    }
+    NC_SET_SMEM_ONCE(tc32_gemm_kernel, TC_SMEM);
     const int shareA = g.A.sbatch == 0, shareB = g.B.sbatch == 0;
     const int bA = shareA ? 1 : g.batch, bB = shareB ? 1 : g.batch;
     const CUtensorMap mAb = make_map(g.A.big, g.Kr, g.M, g.A.ld, g.A.sbatch, bA, TM);

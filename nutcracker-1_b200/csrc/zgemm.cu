@@ -198,11 +198,7 @@ template <int BM, int BN, int BK, int WM, int WN, int STAGES, int OPA, int OPB>
 void launch_cfg(const ZGemmParams& p, cudaStream_t s) {
     typedef ZTile<BM, BN, BK, WM, WN, STAGES, OPA, OPB> T;
     auto kern = zgemm_dmma_kernel<BM, BN, BK, WM, WN, STAGES, OPA, OPB>;
-    static bool configured = false;  // attribute is per-function, per-device-context
-    if (!configured) {
-        NC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM));
-        configured = true;
-    }
+    NC_SET_SMEM_ONCE(kern, T::SMEM);
     dim3 grid(ceil_div(p.N, BN), ceil_div(p.M, BM), p.batch * p.nsplit);
     NC_ARG((long long)p.batch * p.nsplit <= 65535, "zgemm: batch too large");
     kern<<<grid, T::THREADS, T::SMEM, s>>>(p);

@@ -17,4 +17,7 @@ def declared_symbols():
             if name in ("if", "while", "for", "return", "sizeof") or m.group(0).startswith("typedef"):
                 continue
             names.append(name)
+        # exported data: extern T const *a, *b;
+        for m in re.finditer(r"^extern\s+[^;(]*;", src, re.M):
+            names.extend(re.findall(r"\*\s*([A-Za-z_]\w*)", m.group(0)))
     return names

@@ -10,7 +10,8 @@ expected outputs:
 * ``tests/stress.cpp``      TFIM four-lowest-level energies,
 * ``tests/optimizer.cpp``   one-site optimizer mode cases.
 
-Usage:  python tests/golden/make_golden.py [reference_root]
+Usage:  python tests/golden/make_golden.py <reference_root>
+        (or set NUTCRACKER_REFERENCE to the reference checkout)
 The committed JSON is what the tests read; the reference tree is not needed
 at test time.
 """
@@ -21,7 +22,9 @@ import os
 import re
 import sys
 
-ROOT = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+ROOT = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("NUTCRACKER_REFERENCE", "")
+if __name__ == "__main__" and not ROOT:
+    sys.exit("usage: make_golden.py <reference_root>  (or set NUTCRACKER_REFERENCE)")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_kats.json")
 
 

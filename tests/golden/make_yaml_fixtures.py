@@ -37,4 +37,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("NUTCRACKER_REFERENCE", "")
+    if not root:
+        sys.exit("usage: make_yaml_fixtures.py <reference_root>  (or set NUTCRACKER_REFERENCE)")
+    main(root)
