@@ -101,6 +101,16 @@ int nc_gauge_move_dev(int direction, uint32_t bl, uint32_t bm, uint32_t br, uint
 int nc_tc_zgemm_dev(uint32_t M, uint32_t N, uint32_t K, const void* A_dev, const void* B_dev,
                     void* C_dev, int three);
 
+/* No counterpart in the reference; for tests of the failure path.  Sets
+   the time limit of every mbarrier wait in the tcgen05 GEMM (default 2 s,
+   here in nanoseconds, at least 1000) and, when skip_first_load is nonzero,
+   makes tile (0,0,0) of the following GEMMs leave its first K stage
+   unloaded, so that a wait runs out: the kernel then stops issuing, leaves
+   through its final barrier and frees its tensor memory, and the host call
+   reports NC_ERR_TIMEOUT.  Process-wide; restore (2000000000, 0) after use.
+   Returns a status code. */
+int nc_test_tc32_wait(uint64_t wait_ns, int skip_first_load);
+
 /* No counterpart in the reference.  The same H_eff product as
    nc_heff_apply_dev for callers that cannot let the library allocate
    device memory (a fixed memory budget, or code where a cudaMalloc/cudaFree
@@ -267,12 +277,23 @@ void random_projector_matrix_(const uint32_t* projector_length, const uint32_t* 
 int nc_set_krylov_dimension(int m);
 
 /* ---- Level 0: gauge moves and random sites (core.cpp:463-662, 735-757) --
-   The device path uses a Householder-QR gauge (A = P Q with Q row-
-   orthonormal) instead of the reference's SVD polar factor; the normalised
-   and denormalised outputs differ from the reference element-wise by a
-   unitary on the shared bond, and every contraction of the pair (state,
-   energies, environments, overlaps) is identical.  Return 0 on success,
-   a nonzero status otherwise. */
+   norm_denorm_going_left_/right_, norm_for_left_/right_ and
+   form_norm_overlap_tensors_ return the reference's exact polar factor
+   (U V^H of the site matrix's SVD; the neighbour absorbs U S U^H, as
+   zgesdd gives them in core.f95:2708-2960), computed on the device as a
+   Householder QR followed by the QDWH polar iteration on the small square
+   factor.  A rank-deficient site has no unique polar factor; there, and
+   after nc_set_level0_gauge(0), these entry points use the device chain's
+   Householder-QR gauge (A = P Q with Q row-orthonormal): the outputs then
+   differ from the reference element-wise by a unitary on the shared bond,
+   and every contraction of the pair (state, energies, environments,
+   overlaps) is identical.  Return 0 on success, a nonzero status
+   otherwise. */
+
+/* No counterpart in the reference.  Selects the gauge of the Level-0 moves
+   above on this thread: nonzero (default) = exact polar factor, 0 = the
+   faster Householder-QR gauge.  Returns a status code. */
+int nc_set_level0_gauge(int exact_polar);
 
 /* core.cpp:580-589 (norm_denorm_going_left_): site_tensor_to_normalize
    (br,bm,dr) becomes right-normalised, site_tensor_to_denormalize (bm,bl,dl)
@@ -348,6 +369,10 @@ typedef struct {
                                          3xTF32 tensor-core contractions (FP64 Krylov, eigenproblem
                                          and energies), and sweep_until_converged closes with FP64
                                          refinement sweeps to the options' thresholds */
+    uint32_t maximum_sweeps;          /* sweepUntilConverged: 0 (default) sweeps until the energy
+                                         settles, without bound, as base_chain.cpp:112-123 does;
+                                         k > 0: a call that has not settled after k sweeps fails
+                                         with NC_ERR_NUMERIC ("sweeps did not converge") */
 } nc_chain_options;
 
 /* One MPO site (OperatorSite, tensors.hpp:1641-1854): indices (2,nnz)

@@ -249,6 +249,13 @@ int nc_tc_zgemm_dev(uint32_t M, uint32_t N, uint32_t K, const void* A_dev, const
     return g_status;
 }
 
+int nc_test_tc32_wait(uint64_t wait_ns, int skip_first_load) {
+    NC_ABI_BEGIN
+    tc_test_fault((unsigned long long)wait_ns, skip_first_load);
+    NC_ABI_END
+    return g_status;
+}
+
 void compute_expectation_(const uint32_t* bl, const uint32_t* br, const uint32_t* cl, const uint32_t* cr,
                           const uint32_t* d, const nc_complex* L, const nc_complex* S,
                           const uint32_t* nnz, const uint32_t* idx, const nc_complex* W,

@@ -25,7 +25,8 @@ int32_t norm_denorm_going_left_(const uint32_t* bl, const uint32_t* bm, const ui
     const cplx* dB = h.in(B, nbb);
     cplx* oA = h.out(na);
     cplx* oB = h.out(nbb);
-    gauge_left(h.ctx, *bl, *bm, *br, *dl, *dr, dA, dB, oA, oB);
+    if (h.ctx.level0_polar) gauge_left_polar(h.ctx, *bl, *bm, *br, *dl, *dr, dA, dB, oA, oB);
+    else gauge_left(h.ctx, *bl, *bm, *br, *dl, *dr, dA, dB, oA, oB);
     h.back(denormA, oA, na);
     h.back(normB, oB, nbb);
     h.sync();
@@ -43,10 +44,18 @@ int32_t norm_denorm_going_right_(const uint32_t* bl, const uint32_t* bm, const u
     const cplx* dB = h.in(B, nbb);
     cplx* oA = h.out(na);
     cplx* oB = h.out(nbb);
-    gauge_right(h.ctx, *bl, *bm, *br, *dl, *dr, dA, dB, oA, oB);
+    if (h.ctx.level0_polar) gauge_right_polar(h.ctx, *bl, *bm, *br, *dl, *dr, dA, dB, oA, oB);
+    else gauge_right(h.ctx, *bl, *bm, *br, *dl, *dr, dA, dB, oA, oB);
     h.back(normA, oA, na);
     h.back(denormB, oB, nbb);
     h.sync();
+    NC_ABI_END
+    return g_status;
+}
+
+int nc_set_level0_gauge(int exact_polar) {
+    NC_ABI_BEGIN
+    Context::get().level0_polar = exact_polar != 0;
     NC_ABI_END
     return g_status;
 }
@@ -73,7 +82,8 @@ int32_t norm_for_left_(const uint32_t* br, const uint32_t* bl, const uint32_t* d
     const size_t n = (size_t)*br * *bl * *d;
     const cplx* dS = h.in(S, n);
     cplx* o = h.out(n);
-    gauge_right(h.ctx, *bl, *br, 1, *d, 1, dS, nullptr, o, nullptr);
+    if (h.ctx.level0_polar) gauge_right_polar(h.ctx, *bl, *br, 1, *d, 1, dS, nullptr, o, nullptr);
+    else gauge_right(h.ctx, *bl, *br, 1, *d, 1, dS, nullptr, o, nullptr);
     h.back(out, o, n);
     h.sync();
     NC_ABI_END
@@ -87,7 +97,8 @@ int32_t norm_for_right_(const uint32_t* br, const uint32_t* bl, const uint32_t* 
     const size_t n = (size_t)*br * *bl * *d;
     const cplx* dS = h.in(S, n);
     cplx* o = h.out(n);
-    gauge_left(h.ctx, 1, *bl, *br, 1, *d, nullptr, dS, nullptr, o);
+    if (h.ctx.level0_polar) gauge_left_polar(h.ctx, 1, *bl, *br, 1, *d, nullptr, dS, nullptr, o);
+    else gauge_left(h.ctx, 1, *bl, *br, 1, *d, nullptr, dS, nullptr, o);
     h.back(out, o, n);
     h.sync();
     NC_ABI_END
@@ -153,7 +164,8 @@ void form_norm_overlap_tensors_(const uint32_t* bl, const uint32_t* bm, const ui
     cplx* o_l = h.out(n1);
     cplx* o_u = h.out(n1);
     cplx* o_r = h.out(n2);
-    gauge_right(h.ctx, *bl, *bm, *br, *dl, *dr, d1, d2, nS1, o_d2);
+    if (h.ctx.level0_polar) gauge_right_polar(h.ctx, *bl, *bm, *br, *dl, *dr, d1, d2, nS1, o_d2);
+    else gauge_right(h.ctx, *bl, *bm, *br, *dl, *dr, d1, d2, nS1, o_d2);
     overlap_site_from_state(h.ctx, *bm, *bl, *dl, d1, o_u);
     overlap_site_from_state(h.ctx, *bm, *bl, *dl, nS1, o_l);
     overlap_site_from_state(h.ctx, *br, *bm, *dr, d2, o_r);

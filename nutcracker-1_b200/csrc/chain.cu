@@ -110,8 +110,6 @@ struct ProjSite {
     int bl = 0, br = 0, d = 0;
 };
 
-constexpr int kMaxSweeps = 500;
-
 // Diagnostic phase timer: synchronises the stream on entry and exit and adds
 // the wall time to `acc` (only when the chain's time_phases option is set).
 struct PhaseTimer {
@@ -621,10 +619,13 @@ struct Chain {
         double prev = energy;
         perform_optimization_sweep();
         double now = energy;
-        int count = 1;
+        uint64_t count = 1;
         while (outside_tolerance(prev, now, opt.sweep_convergence_threshold)) {
-            // the reference loops without bound; cap it so a stalled chain returns an error
-            if (++count > kMaxSweeps) throw Error(NC_ERR_NUMERIC, "sweeps did not converge");
+            // the reference loops without bound (slow linear convergence of a
+            // level at a small bond dimension can take ~1000 sweeps at the
+            // 1e-12 default); maximum_sweeps, when set, turns that into an error
+            if (opt.maximum_sweeps && ++count > opt.maximum_sweeps)
+                throw Error(NC_ERR_NUMERIC, "sweeps did not converge");
             perform_optimization_sweep();
             prev = now;
             now = energy;
@@ -819,6 +820,7 @@ ChainOptions to_options(const nc_chain_options* o) {
     c.strict = o->strict != 0;
     c.time_phases = o->time_phases != 0;
     c.precision = (int)o->precision;
+    c.maximum_sweeps = o->maximum_sweeps;
     return c;
 }
 }  // namespace

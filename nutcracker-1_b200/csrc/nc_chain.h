@@ -37,6 +37,7 @@ struct ChainOptions {
     bool strict = false;                // raise on a site failure instead of keeping the old site
     bool time_phases = false;           // synchronise and time each phase
     int precision = 0;                  // 0: all FP64; 1: precision form (mixed sweeps + FP64 refinement)
+    uint32_t maximum_sweeps = 0;        // sweep_until_converged bound per call; 0 = none (the reference's loop)
 };
 
 // Thresholds of the mixed sweeps (the FP64 refinement uses the options'):

@@ -98,6 +98,10 @@ struct Context {
     size_t pinned_bytes = 0;
     uint64_t launches = 0;   // kernels launched by this library on this context
     int krylov_dim = 24;     // Lanczos basis size before a restart
+    // Gauge of the Level-0 norm_denorm_* / norm_for_* entry points: true
+    // (default) = the reference's exact polar factor, false = the faster
+    // Householder-QR gauge (the same state, a different site tensor).
+    bool level0_polar = true;
     // Workspace arena for GEMM split-K partials and QR scratch: the context
     // arena, or a captured graph's private arena while it is being recorded.
     Arena* ws_override = nullptr;
@@ -115,6 +119,13 @@ struct Context {
     std::vector<double> prof_flops;
     std::vector<int> prof_kind;   // 0: FP64 DMMA complex GEMM, 1: tcgen05 3xTF32 GEMM
     size_t prof_used = 0;
+    // Host waits on this context's stream: spin (cudaStreamSynchronize, the
+    // lowest latency) by default; a blocking-sync event when many threads
+    // share the host's cores (the serving engine's workers), so that waiting
+    // threads leave the cores to the ones launching work.
+    bool blocking_sync = false;
+    cudaEvent_t sync_event = nullptr;
+    void sync();
     Context();
     ~Context();
     static Context& get();   // thread-local default context

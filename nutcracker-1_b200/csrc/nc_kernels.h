@@ -170,6 +170,9 @@ struct TcGemm {
 void tc_gemm(Context& ctx, const TcGemm& g);
 // Synchronises ctx.stream; raises NC_ERR_TIMEOUT if a tc32 pipeline wait expired.
 void tc_check(Context& ctx);
+// Test hook: the limit of every tc32 mbarrier wait (ns) and the switch that
+// leaves the first K stage of tile (0,0,0) unloaded (its wait then runs out).
+void tc_test_fault(unsigned long long wait_ns, int skip_first_load);
 
 // ---- precision form of the site products (mixed.cu) ------------------------
 // Tensor-core operands of one site's H_eff (environments expanded once per
@@ -212,6 +215,17 @@ void gauge_right(Context& ctx, int bl, int bm, int br, int dl, int dr, const cpl
 // B (br,bm,dr) -> normB right-normalised; A (bm,bl,dl) absorbs the factor.
 void gauge_left(Context& ctx, int bl, int bm, int br, int dl, int dr, const cplx* A, const cplx* B,
                 cplx* denormA, cplx* normB, const AbsorbAsync* async = nullptr);
+// The same moves with the reference's exact polar factor (polar.cu): the
+// normalised site is U V^H of the site matrix's SVD and the neighbour absorbs
+// U S U^H, as zgesdd gives them (core.f95:2708-2960); a rank-deficient site
+// falls back to the QR gauge above.
+void gauge_right_polar(Context& ctx, int bl, int bm, int br, int dl, int dr, const cplx* A, const cplx* B,
+                       cplx* normA, cplx* denormB);
+void gauge_left_polar(Context& ctx, int bl, int bm, int br, int dl, int dr, const cplx* A, const cplx* B,
+                      cplx* denormA, cplx* normB);
+// Polar decomposition A = U H of a square n x n matrix (n <= 1024) by QDWH;
+// false if it did not converge to an isometry (A rank-deficient).
+bool polar_qdwh(Context& ctx, int n, const cplx* A, cplx* U, cplx* H);
 void rand_norm_site(Context& ctx, int br, int bl, int d, uint64_t seed, cplx* out);
 void rand_unnorm_site(Context& ctx, int br, int bl, int d, uint64_t seed, cplx* out);
 void increase_bandwidth(Context& ctx, int bl, int bm, int br, int dl, int dr, int new_bm, uint64_t seed,

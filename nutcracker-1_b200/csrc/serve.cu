@@ -82,6 +82,9 @@ struct nc_server {
 
 void nc_server::worker() {
     cudaSetDevice(device);
+    // Many workers share the host's cores: their waits block instead of
+    // spinning, so the threads that are launching work keep the cores.
+    nc::Context::get().blocking_sync = true;
     for (;;) {
         Request* r = nullptr;
         {

@@ -51,9 +51,17 @@ constexpr int TC_THREADS = 64 + 32 * EPI_WARPS;
 constexpr int TMEM_COLS = 512;       // two accumulator buffers of TN columns
 constexpr int CHUNK_KB = 2;          // K stages (per segment) per accumulator chunk
 constexpr size_t TC_SMEM = (size_t)STAGES * STAGE_BYTES + 1024 + 256;
-constexpr unsigned long long WAIT_NS = 2000000000ull;   // 2 s per wait
 
 __device__ int g_tc_error = 0;
+// Limit of every mbarrier wait (2 s by default), and a test switch under
+// which tile (0,0,0) leaves its first K stage unloaded, so that its MMA
+// issuer's wait for that stage runs out and the failure path (g_tc_error,
+// NC_ERR_TIMEOUT on the host) can be exercised without a fault: every other
+// wait is bounded as well, no MMA has been issued, and the loads that were
+// issued complete long before the waits expire.  Both are set only by
+// tc_test_fault (nc_test_tc32_wait).
+__device__ unsigned long long g_tc_wait_ns = 2000000000ull;
+__device__ int g_tc_skip_first_load = 0;
 
 struct TcParams {
     int M, Nr, Kr, nkb;      // nkb: K stages per segment
@@ -82,12 +90,12 @@ __device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait: false (and g_tc_error set) when the phase did not complete in WAIT_NS.
-__device__ __noinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+// Bounded wait: false (and g_tc_error set) when the phase did not complete in `limit` ns.
+__device__ __noinline__ bool mbar_wait(uint32_t bar, uint32_t parity, unsigned long long limit) {
     if (mbar_test(bar, parity)) return true;
     const unsigned long long t0 = gtimer();
     while (!mbar_test(bar, parity)) {
-        if (gtimer() - t0 > WAIT_NS) {
+        if (gtimer() - t0 > limit) {
             atomicExch(&g_tc_error, 1);
             return false;
         }
@@ -164,6 +172,7 @@ tc32_gemm_kernel(const __grid_constant__ CUtensorMap mapAb, const __grid_constan
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.x * TM, n0 = blockIdx.y * TN, z = blockIdx.z;
+    const unsigned long long limit = g_tc_wait_ns;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
@@ -193,6 +202,7 @@ tc32_gemm_kernel(const __grid_constant__ CUtensorMap mapAb, const __grid_constan
     if (warp == 0) {
         if (lane == 0) {
             const int zA = P.shareA ? 0 : z, zB = P.shareB ? 0 : z;
+            const bool skip_first = g_tc_skip_first_load && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0;
             int t = 0;
             bool ok = true;
             for (int c = 0; c < nchunk && ok; ++c) {
@@ -201,7 +211,8 @@ tc32_gemm_kernel(const __grid_constant__ CUtensorMap mapAb, const __grid_constan
                     for (int kb = kb0; kb < kb1; ++kb, ++t) {
                         const int s = t % STAGES;
                         const uint32_t ph = (uint32_t)(t / STAGES) & 1u;
-                        if (!mbar_wait(empty0 + 8 * s, ph ^ 1u)) { ok = false; break; }
+                        if (!mbar_wait(empty0 + 8 * s, ph ^ 1u, limit)) { ok = false; break; }
+                        if (skip_first && t == 0) continue;   // test switch: stage 0 never arrives
                         const CUtensorMap* ma = (seg == 2) ? &mapAs : &mapAb;
                         const CUtensorMap* mb = (seg == 1) ? &mapBs : &mapBb;
                         mbar_expect_tx(full0 + 8 * s, STAGE_BYTES);
@@ -217,7 +228,7 @@ tc32_gemm_kernel(const __grid_constant__ CUtensorMap mapAb, const __grid_constan
             for (int c = 0; c < nchunk && ok; ++c) {
                 const int b = c & 1;
                 const uint32_t acc = tmem_d + (uint32_t)(b * TN);
-                if (!mbar_wait(acce0 + 8 * b, ((uint32_t)(c >> 1) & 1u) ^ 1u)) break;   // buffer drained
+                if (!mbar_wait(acce0 + 8 * b, ((uint32_t)(c >> 1) & 1u) ^ 1u, limit)) break;   // buffer drained
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const int kb0 = c * CHUNK_KB, kb1 = min(P.nkb, kb0 + CHUNK_KB);
                 bool first = true;
@@ -225,7 +236,7 @@ tc32_gemm_kernel(const __grid_constant__ CUtensorMap mapAb, const __grid_constan
                     for (int kb = kb0; kb < kb1; ++kb, ++t) {
                         const int s = t % STAGES;
                         const uint32_t ph = (uint32_t)(t / STAGES) & 1u;
-                        if (!mbar_wait(full0 + 8 * s, ph)) { ok = false; break; }
+                        if (!mbar_wait(full0 + 8 * s, ph, limit)) { ok = false; break; }
                         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                         const uint64_t da = smem_desc(base + s * STAGE_BYTES);
                         const uint64_t db = smem_desc(base + s * STAGE_BYTES + A_STAGE);
@@ -250,7 +261,7 @@ tc32_gemm_kernel(const __grid_constant__ CUtensorMap mapAb, const __grid_constan
         bool ok = true;
         for (int c = 0; c < nchunk; ++c) {
             const int b = c & 1;
-            ok = __all_sync(0xffffffffu, mbar_wait(accf0 + 8 * b, (uint32_t)(c >> 1) & 1u));   // warp-uniform
+            ok = __all_sync(0xffffffffu, mbar_wait(accf0 + 8 * b, (uint32_t)(c >> 1) & 1u, limit));   // warp-uniform
             if (!ok) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
@@ -350,6 +361,12 @@ void tc_gemm(Context& ctx, const TcGemm& g) {
         NC_CHECK_LAUNCH();
     });
     ctx.launches++;
+}
+
+void tc_test_fault(unsigned long long wait_ns, int skip_first_load) {
+    NC_ARG(wait_ns >= 1000, "tc32 wait limit must be at least 1 microsecond");
+    NC_CUDA(cudaMemcpyToSymbol(g_tc_wait_ns, &wait_ns, sizeof(wait_ns)));
+    NC_CUDA(cudaMemcpyToSymbol(g_tc_skip_first_load, &skip_first_load, sizeof(int)));
 }
 
 void tc_check(Context& ctx) {

@@ -95,7 +95,19 @@ unsigned* Context::reduction_counter() {
     return red_counter;
 }
 
+void Context::sync() {
+    if (!blocking_sync) {
+        NC_CUDA(cudaStreamSynchronize(stream));
+        return;
+    }
+    if (!sync_event)
+        NC_CUDA(cudaEventCreateWithFlags(&sync_event, cudaEventBlockingSync | cudaEventDisableTiming));
+    NC_CUDA(cudaEventRecord(sync_event, stream));
+    NC_CUDA(cudaEventSynchronize(sync_event));
+}
+
 Context::~Context() {
+    if (sync_event) cudaEventDestroy(sync_event);
     if (red_counter) cudaFree(red_counter);
     if (own_stream) cudaStreamDestroy(own_stream);
     if (pinned) cudaFreeHost(pinned);
@@ -286,7 +298,7 @@ void znormalize_dev(Context& ctx, long long n, const cplx* nrm2sq_dev, cplx* x) 
 void read_scalars(Context& ctx, const void* dev, size_t bytes, void* host) {
     NC_ARG(bytes <= ctx.pinned_bytes, "read_scalars: too many bytes");
     NC_CUDA(cudaMemcpyAsync(ctx.pinned, dev, bytes, cudaMemcpyDeviceToHost, ctx.stream));
-    NC_CUDA(cudaStreamSynchronize(ctx.stream));
+    ctx.sync();
     memcpy(host, ctx.pinned, bytes);
 }
 

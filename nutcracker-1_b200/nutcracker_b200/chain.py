@@ -29,6 +29,7 @@ class nc_chain_options(ct.Structure):
         ("strict", ct.c_uint32),
         ("time_phases", ct.c_uint32),
         ("precision", ct.c_uint32),
+        ("maximum_sweeps", ct.c_uint32),
     ]
 
 

@@ -437,7 +437,7 @@ def _strategy_1(bl, br, cl, cr, d, L, idx, W, R, proj, which):
 
 
 def optimize(bl, br, cl, cr, d, L, idx, W, R, nproj, nrefl, orth_dim, reflectors, tau,
-             swaps, which, tol, maxit, guess, heff=None):
+             swaps, which, tol, maxit, guess, heff=None, ncv0=3):
     """core.f95:1911-2047 (dispatcher) with strategies 1-3.
 
     Returns (info, iterations, eigenvalue, result (br,bl,d), normal).  ARPACK
@@ -446,6 +446,11 @@ def optimize(bl, br, cl, cr, d, L, idx, W, R, nproj, nrefl, orth_dim, reflectors
     supplies the full-space H_eff product (used by the CPU baseline to time the
     reference's matrix-free ordering); by default strategy 3 uses the
     reference ordering (iteration_stage_1 once, stages 2 and 3 per product).
+    ``ncv0`` is ARPACK's first basis size: 3 in the reference
+    (core.f95:2565); a larger value changes only how much work ARPACK does to
+    reach the same tolerance (a 3-vector basis at tol 1e-12 takes thousands
+    of restarts per site at bond dimension 64), which the at-scale parity
+    tests use to finish in minutes.
     """
     n = d * bl * br
     which = which.decode() if isinstance(which, bytes) else which
@@ -495,7 +500,7 @@ def optimize(bl, br, cl, cr, d, L, idx, W, R, nproj, nrefl, orth_dim, reflectors
         j = int(np.argmin(np.real(w)))  # core.f95:2523
         return w[j], v[:, j]
 
-    ncv = 3
+    ncv = min(ncv0, orth_dim)
     got = run(ncv)
     if got is None:
         if n < maxit:

@@ -194,6 +194,10 @@ class ChainOptions:
     initial_bandwidth_dimension: int = 1
     compute_new_bandwidth_dimension: Callable[[int], int] = lambda b: b + 1
     optimizer_mode: str = "<v"
+    # ARPACK's basis size; the reference fixes 3 (core.f95:2565).  Not a
+    # reference option: larger values reach the same converged states with
+    # fewer restarts, for oracle runs at bond dimension 64 and above.
+    arpack_ncv: int = 3
 
 
 # ---------------------------------------------------------------------------
@@ -234,7 +238,7 @@ def overlap_with_projectors(pm, S):
                                                 pm.swaps, S.size, S)
 
 
-def optimize_state_site(L, S, op, R, pm, tol, sanity, maxit, mode):
+def optimize_state_site(L, S, op, R, pm, tol, sanity, maxit, mode, ncv=3):
     """optimizer.cpp:201-315."""
     br, bl, d = S.shape
     which = MODES[mode][0]
@@ -243,7 +247,7 @@ def optimize_state_site(L, S, op, R, pm, tol, sanity, maxit, mode):
     else:
         args = (0, 0, S.size, None, None, None)
     status, iters, ev, new, normal = core.optimize(bl, br, op.cl, op.cr, d, L, op.idx, op.W, R,
-                                                   *args, which, tol, maxit, S)
+                                                   *args, which, tol, maxit, S, ncv0=ncv)
     expectation = compute_expectation_value_at_site(L, new, op, R)
     overlap = overlap_with_projectors(pm, new)
     if status == -14:
@@ -356,6 +360,26 @@ class InitialSiteSource:
 
     def middle(self, d, bl, br):
         return core.rand_unnorm_state_site_tensor(br, bl, d, self.rng)
+
+
+class ReplaySource:
+    """A given state as the chain's initial sites: ``sites`` (br, bl, d), site 0
+    the centre, the rest right-normalised (the layout ``state_sites`` returns),
+    handed out in the order ``Chain.reset`` draws them (sites N-1 .. 1, then
+    the centre).  Used to run the oracle from the device chain's state."""
+
+    def __init__(self, sites):
+        self.rights = [np.asfortranarray(s) for s in sites[1:]]
+        self.centre = np.asfortranarray(sites[0])
+
+    def right(self, d, bl, br):
+        s = self.rights.pop()  # site N-1 first
+        assert s.shape == (br, bl, d), (s.shape, (br, bl, d))
+        return s
+
+    def middle(self, d, bl, br):
+        assert self.centre.shape == (br, bl, d), (self.centre.shape, (br, bl, d))
+        return self.centre
 
 
 @dataclass
@@ -482,7 +506,7 @@ class Chain:
             iters, ev, new = optimize_state_site(
                 self.left_exp, self.state_site, self.ops[self.current], self.right_exp, self.pm,
                 o.site_convergence_threshold, o.sanity_check_threshold,
-                o.maximum_number_of_iterations, o.optimizer_mode)
+                o.maximum_number_of_iterations, o.optimizer_mode, o.arpack_ncv)
             if MODES[o.optimizer_mode][1](self.energy, ev, o.sanity_check_threshold):
                 raise OptimizerObtainedRegressiveEigenvalue(self.energy, ev)
             if ((self.energy >= 0 and ev >= 0) or (self.energy <= 0 and ev <= 0)

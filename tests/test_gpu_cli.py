@@ -39,6 +39,29 @@ def test_piped_four_levels_match_reference_energies():
         assert abs(e - ref) <= 1e-7 * abs(ref), (levels, REF)
 
 
+@pytest.mark.parametrize("fixture,levels", [
+    ("external_field_5.yaml", 4),           # README:25  external-field.py 5 | nutcracker -n 4
+    ("transverse_ising_0.1_6.yaml", 3),     # README:32  transverse-ising-model.py 0.1 6 | nutcracker -n 3
+    ("transverse_ising_0.1_10.yaml", 4),    # the ten-site chain of tests/stress.cpp, four levels
+])
+def test_readme_commands_at_default_options(fixture, levels):
+    """No options at all: the reference's defaults (chain_options.cpp:21-30:
+    initial bond dimension 1, every threshold 1e-12), sweeps until converged
+    without a sweep bound as base_chain.cpp:112-123 does.  Energies against
+    exact diagonalisation of the same YAML operator (1e-9 relative)."""
+    from nutcracker_b200 import yaml_io
+    from oracle import ed
+
+    text = open(os.path.join(ROOT, "tests", "golden", "yaml", fixture), "rb").read()
+    r = run(["-n", str(levels)], stdin=text)
+    assert r.returncode == 0, r.stderr
+    got = yaml.safe_load(r.stdout)["Energy levels"]
+    assert len(got) == levels, r.stderr
+    want, _ = ed.lowest_levels(yaml_io.read_operator(text), levels)
+    for g, e in zip(got, want):
+        assert abs(g - e) <= 1e-9 * max(abs(e), 1.0), (got, list(want))
+
+
 def test_file_input_location_output_file_and_overwrite(tmp_path):
     nested = "problem:\n  hamiltonian:\n" + "".join(
         "    " + line + "\n" for line in open(TFIM).read().splitlines() if line and not line.startswith("---"))

@@ -1,11 +1,16 @@
 """GPU parity: gauge moves, bandwidth growth, random sites, projector sites.
 
-The device gauge is a Householder-QR factor instead of the reference's SVD
-polar factor (core.f95:2708-2960), so outputs are compared through the
-gauge-invariant quantities the reference's own tests use (tests/states.cpp,
+The Level-0 gauge entry points return the reference's exact polar factor
+(core.f95:2708-2960: U V^H of the SVD, the neighbour absorbing U S U^H), so
+their outputs are compared element-wise with the oracle's zgesdd-based
+moves (1e-10 relative: the polar factor of these random sites is
+conditioned to ~1e3).  The device chain's Householder-QR gauge (selected
+with nc_set_level0_gauge(0)) is compared through the gauge-invariant
+quantities the reference's own tests use (tests/states.cpp,
 tests/chain.cpp:143-169): the contracted two-site tensor, orthonormality of
 the normalised site, and the state itself.  Tolerance 1e-12 relative.
 """
+import ctypes as ct
 import numpy as np
 import pytest
 
@@ -53,9 +58,11 @@ def test_norm_denorm_going_right(nb, dims):
     assert info == 0
     assert left_normal_err(nA) < 1e-12
     assert rel_err(pair(nA, dB), pair(A, B)) < 1e-12
-    # same state as the reference's polar move
+    # the reference's polar move, element by element
     _, rA, rB = core.norm_denorm_going_right(bl, bm, br, dl, dr, A, B)
     assert rel_err(pair(nA, dB), pair(rA, rB)) < 1e-12
+    assert rel_err(nA, rA) < 1e-10
+    assert rel_err(dB, rB) < 1e-10
 
 
 @pytest.mark.parametrize("dims", DIMS, ids=lambda d: "x".join(map(str, d)))
@@ -69,6 +76,43 @@ def test_norm_denorm_going_left(nb, dims):
     assert info == 0
     assert right_normal_err(nB) < 1e-12
     assert rel_err(pair(dA, nB), pair(A, B)) < 1e-12
+    _, rA, rB = core.norm_denorm_going_left(bl, bm, br, dl, dr, A, B)
+    assert rel_err(dA, rA) < 1e-10
+    assert rel_err(nB, rB) < 1e-10
+
+
+@pytest.mark.parametrize("dims", [(8, 12, 3), (40, 30, 2), (64, 128, 2), (300, 200, 3)],
+                         ids=lambda d: "x".join(map(str, d)))
+def test_norm_for_left_right_polar(nb, dims):
+    """core.f95:2880-2960: the polar factor alone, element by element."""
+    br, bl, d = dims
+    rng = np.random.default_rng(br + 3 * bl)
+    S = rand_c(rng, (br, bl, d))
+    if bl * d >= br:
+        info, got = nb.Core.norm_for_left(br, bl, d, S)
+        assert info == 0
+        assert rel_err(got, core.norm_for_left(br, bl, d, S)[1]) < 1e-10
+    if br * d >= bl:
+        info, got = nb.Core.norm_for_right(br, bl, d, S)
+        assert info == 0
+        assert rel_err(got, core.norm_for_right(br, bl, d, S)[1]) < 1e-10
+
+
+def test_qr_gauge_option(nb):
+    """nc_set_level0_gauge(0): the device chain's QR gauge, same state."""
+    bl, bm, br, dl, dr = 64, 100, 64, 2, 2
+    rng = np.random.default_rng(5)
+    A = rand_c(rng, (bm, bl, dl)); B = rand_c(rng, (br, bm, dr))
+    assert nb.lib.nc_set_level0_gauge(ct.c_int(0)) == 0
+    try:
+        info, nA, dB = nb.Core.norm_denorm_going_right(bl, bm, br, dl, dr, A, B)
+    finally:
+        assert nb.lib.nc_set_level0_gauge(ct.c_int(1)) == 0
+    assert info == 0
+    _, rA, rB = core.norm_denorm_going_right(bl, bm, br, dl, dr, A, B)
+    assert left_normal_err(nA) < 1e-12
+    assert rel_err(pair(nA, dB), pair(rA, rB)) < 1e-12
+    assert rel_err(nA, rA) > 1e-3   # a different gauge
 
 
 def test_rank_deficient_gauge(nb):
@@ -128,6 +172,8 @@ def test_form_norm_overlap_tensors(nb):
     # the left-normalised overlap site and the denormalised site 2 carry the same pair
     back = lambda O: np.conj(np.transpose(O, (2, 0, 1)))  # overlap (bl,d,br) -> state (br,bl,d)
     assert rel_err(pair(back(lno), dS2), pair(back(rl), rd)) < 1e-12
+    # with the exact polar factor, element by element
+    assert rel_err(lno, rl) < 1e-10 and rel_err(dS2, rd) < 1e-10
 
 
 @pytest.mark.parametrize("direction", [1, -1])

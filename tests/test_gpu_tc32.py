@@ -111,3 +111,31 @@ def test_mixed_environment_matches_fp64(side, bl, br):
     torch.cuda.synchronize()
     err = _rel(omx, o64)
     assert err <= TOL_3X, err
+
+
+def test_bounded_wait_reports_timeout_and_context_recovers():
+    """The failure path of the tcgen05 GEMM's bounded waits, without a fault:
+    with the test switch, tile (0,0,0) leaves its first K stage unloaded, its
+    MMA issuer's wait runs out after the (shortened, 2 ms) limit, the kernel
+    stops issuing, frees its tensor memory and returns, and the host call
+    reports NC_ERR_TIMEOUT (1004).  The next GEMM on the same context, with
+    the default limit restored, is correct."""
+    import torch
+
+    import nutcracker_b200 as nb
+
+    M, N, K = 128, 128, 64
+    g = torch.Generator(device="cuda").manual_seed(5)
+    A_cm = torch.randn(K, M, dtype=torch.complex128, device="cuda", generator=g)
+    B_cm = torch.randn(N, K, dtype=torch.complex128, device="cuda", generator=g)
+    C_cm = torch.zeros((N, M), dtype=torch.complex128, device="cuda")
+    assert nb.lib.nc_test_tc32_wait(ct.c_uint64(2_000_000), 1) == 0
+    try:
+        st = nb.lib.nc_tc_zgemm_dev(M, N, K, _p(A_cm), _p(B_cm), _p(C_cm), 1)
+    finally:
+        assert nb.lib.nc_test_tc32_wait(ct.c_uint64(2_000_000_000), 0) == 0
+    assert st == 1004, (st, nb.lib.nc_last_error())
+    assert b"time limit" in nb.lib.nc_last_error()
+    st = nb.lib.nc_tc_zgemm_dev(M, N, K, _p(A_cm), _p(B_cm), _p(C_cm), 1)
+    assert st == 0, nb.lib.nc_last_error()
+    assert _rel(C_cm.T, A_cm.T @ B_cm.T) <= TOL_3X
