@@ -178,8 +178,9 @@ def test_form_norm_overlap_tensors(nb):
 
 @pytest.mark.parametrize("direction", [1, -1])
 def test_gauge_move_dev_matches_host_entry(nb, direction):
-    """nc_gauge_move_dev (device pointers) gives the host entry points' results
-    bit for bit, and leaves its inputs unchanged."""
+    """nc_gauge_move_dev (device pointers, the chain's QR gauge) gives the host
+    entry points' results in their QR mode (nc_set_level0_gauge(0)) bit for
+    bit, and leaves its inputs unchanged."""
     import ctypes as ct
 
     import torch
@@ -187,10 +188,14 @@ def test_gauge_move_dev_matches_host_entry(nb, direction):
     bl, bm, br, dl, dr = 256, 300, 256, 2, 2
     rng = np.random.default_rng(5 + direction)
     A = rand_c(rng, (bm, bl, dl)); B = rand_c(rng, (br, bm, dr))
-    if direction > 0:
-        _, wantA, wantB = nb.Core.norm_denorm_going_right(bl, bm, br, dl, dr, A, B)
-    else:
-        _, wantA, wantB = nb.Core.norm_denorm_going_left(bl, bm, br, dl, dr, A, B)
+    assert nb.lib.nc_set_level0_gauge(ct.c_int(0)) == 0
+    try:
+        if direction > 0:
+            _, wantA, wantB = nb.Core.norm_denorm_going_right(bl, bm, br, dl, dr, A, B)
+        else:
+            _, wantA, wantB = nb.Core.norm_denorm_going_left(bl, bm, br, dl, dr, A, B)
+    finally:
+        assert nb.lib.nc_set_level0_gauge(ct.c_int(1)) == 0
     dA = torch.from_numpy(A.ravel(order="F").copy()).cuda()
     dB = torch.from_numpy(B.ravel(order="F").copy()).cuda()
     oA, oB = torch.empty_like(dA), torch.empty_like(dB)
