@@ -516,6 +516,90 @@ int nc_server_get_stats(nc_server* server, nc_server_stats* stats);
 /* Finishes the queued requests, stops the workers and frees the server. */
 void nc_server_free(nc_server* server);
 
+/* ---- Batched form (no counterpart in the reference) ----------------------
+
+   Many independent chains (each its own operator, number of sites and bond
+   dimension) swept in lockstep on one GPU.  Every chain runs the reference's
+   single-site sweep (chain.cpp:147-163) until its sweep energy settles
+   (base_chain.cpp:112-123); the per-site work is that of optimize_
+   (core.f95:2131-2609) and contract_sos_left/right (core.f95:623-848).
+   Each contraction stage of all chains' site solves, gauge moves and
+   environment updates is one persistent launch over a work list spanning
+   the chains; the tile shape of every problem comes from a table keyed by
+   (stage, bond dimension, MPO bond dimension, physical dimension) that the
+   autotuner below fills.  A Lanczos iteration of every chain is one CUDA
+   graph replay.  The chains start from seeded random states (one seed per
+   chain), every reduction runs in a fixed order within its chain, so a
+   chain's energies are the same alone and in any batch.  Ground states only
+   (no projectors). */
+typedef struct {
+    uint32_t precision;               /* 1 (default): contractions in complex FP32 (complex64 products;
+                                         FP64 Krylov basis, reorthogonalisation, projected problem,
+                                         gauge moves and energies), sweeps until the relative energy
+                                         change is below 1e-7 (at most 50); 0: FP64 throughout */
+    uint32_t refine;                  /* precision 1: then rebuild every environment in FP64 and sweep
+                                         in FP64 to sweep_convergence_threshold (default 1) */
+    uint32_t krylov_dimension;        /* Lanczos basis before an explicit restart, 2..24 (default 16) */
+    uint32_t maximum_number_of_iterations;   /* restarts before a site solve fails (default 100) */
+    double sanity_check_threshold;    /* acceptance rule of base_chain.cpp:97-103 (default 1e-12) */
+    double site_convergence_threshold;   /* Ritz residual <= tol * |theta| (default 1e-12) */
+    double sweep_convergence_threshold;  /* relative sweep-energy change (default 1e-12) */
+    uint32_t maximum_sweeps;          /* FP64 sweeps per chain, 0 (default): no bound; a chain that
+                                         reaches it stops and reports converged = 0 */
+    uint64_t seed;                    /* seed of every chain when no per-chain seeds are given */
+} nc_batch_options;
+typedef struct {
+    double energy;                    /* the last accepted site energy of the final sweep */
+    uint32_t sweeps, mixed_sweeps, fp64_sweeps;
+    uint32_t converged;               /* 0: stopped by maximum_sweeps */
+    uint32_t bandwidth_dimension, reserved;
+    uint64_t site_solves;
+} nc_batch_chain_result;
+typedef struct {
+    uint32_t chains, reserved;
+    uint64_t global_steps;            /* lockstep actions (each: moves of the chains that move, then
+                                         a site solve of every chain still sweeping) */
+    uint64_t lanczos_iterations;      /* Lanczos graph replays (one iteration of every chain) */
+    uint64_t graph_launches;
+    uint64_t kernel_launches;         /* kernels launched, graph nodes included */
+    uint64_t device_bytes;            /* the batch's device allocation */
+    double seconds;                   /* wall time of the last nc_batch_solve */
+} nc_batch_stats;
+typedef struct nc_batch nc_batch;
+
+void nc_batch_options_init(nc_batch_options* options);
+/* Copies every chain's operator to the device and allocates all of the
+   batch's device memory (one allocation; nothing is allocated while it
+   solves).  sites[c] points at chain c's number_of_sites[c] operator sites;
+   bandwidth_dimensions[c] is its bond dimension (bond dimension x physical
+   dimension <= 512); seeds may be NULL (options->seed for every chain).
+   NULL on error. */
+nc_batch* nc_batch_create(uint32_t number_of_chains, const uint32_t* number_of_sites,
+                          const nc_operator_site* const* sites, const uint32_t* bandwidth_dimensions,
+                          const uint64_t* seeds, const nc_batch_options* options);
+void nc_batch_free(nc_batch* batch);
+/* Tile table: `count` entries of five int32 (stage, bond dimension, MPO bond
+   dimension, physical dimension, tile configuration); a problem takes the
+   entry of its stage, MPO and physical dimension whose bond dimension is
+   nearest its own (power-of-two buckets), else a size rule.  Stages: 0 H_eff
+   first product, 1 H_eff last product, 2 left environment, 3 and 4 right
+   environment, 5 gauge-factor absorption. */
+int nc_batch_set_tile_table(nc_batch* batch, const int32_t* entries, uint32_t count);
+/* Random initial states, then sweeps until every chain has settled. */
+int nc_batch_solve(nc_batch* batch);
+/* One result per chain, in creation order. */
+int nc_batch_get_results(nc_batch* batch, nc_batch_chain_result* results);
+int nc_batch_get_stats(nc_batch* batch, nc_batch_stats* stats);
+/* Autotuner measurement: seconds per launch of one grouped launch holding
+   `problems` copies of `stage`'s interior-site products at (bond dimension
+   chi, MPO bond dimension D, physical dimension d), for each tile
+   configuration (nc_batch_tile_configs entries). */
+int nc_batch_autotune_stage(uint32_t stage, uint32_t chi, uint32_t D, uint32_t d, uint32_t problems,
+                            uint32_t reps, uint32_t precision, double* seconds_per_config);
+/* Number of tile configurations; rows/cols (may be NULL) receive their output
+   tile shapes. */
+uint32_t nc_batch_tile_configs(int32_t* rows, int32_t* cols);
+
 /* ---- YAML operator format (yaml.cpp:169-306, README:27-187) ----------------
    The input format of the reference's `nutcracker` program: a "sites" list of
    {physical dimension, left dimension, right dimension, matrices: [{from, to,
