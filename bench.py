@@ -51,6 +51,15 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "nutcracker-1_b200"))
 
+T_START = time.perf_counter()
+
+
+def log(msg):
+    """Progress line on stderr (the JSON line alone goes to stdout)."""
+    sys.stderr.write("[bench %7.1fs] %s\n" % (time.perf_counter() - T_START, msg))
+    sys.stderr.flush()
+
+
 METRIC = "sweeps/s @N=100 \u03c7=1024 mixed vs FP64 GPU at |\u0394E|/N\u22641e-9"
 UNIT = "sweeps/s"
 # H_eff products per interior site step charged to the CPU sample when no
@@ -89,7 +98,8 @@ def parse():
                     help="requests of the stream timed one at a time and then all at once (the plain "
                          "per-solve baseline and the concurrency speed-up on the same requests)")
     ap.add_argument("--serve-slots", type=int, default=0, help="concurrent requests (0: min(32, 2 x cores))")
-    ap.add_argument("--serve-rate", type=float, default=64.0, help="Poisson arrival rate, requests/s")
+    ap.add_argument("--serve-rates", default="4,64",
+                    help="Poisson arrival rates swept by the serving sample, requests/s (comma-separated)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-form sample")
     ap.add_argument("--no-config3", action="store_true", help="skip the spin-1 precision-form sample")
     ap.add_argument("--config3-only", action="store_true", help="run only the spin-1 precision-form sample")
@@ -97,8 +107,10 @@ def parse():
     ap.add_argument("--c3-chi", type=int, default=512)
     ap.add_argument("--c3-levels", type=int, default=2)
     ap.add_argument("--batched-only", action="store_true", help="run only the batched-form sample")
-    ap.add_argument("--batch-chains", type=int, default=16,
+    ap.add_argument("--batch-chains", type=int, default=256,
                     help="chains in the batched sample (the batched workload has 4096; a bounded sample)")
+    ap.add_argument("--batch-plain", type=int, default=16,
+                    help="chains of the batch also solved one at a time by the single-chain engine")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-cpu-validation", action="store_true",
                     help="skip the oracle's measured chi=128 sweep segment that checks the extrapolation model")
@@ -220,13 +232,15 @@ def serving_sample(args):
     dimension), 1-4 levels each, seeded, Poisson arrivals, in the plain FP64 form and in the
     precision form (precision=1: mixed sweeps and the FP64 refinement).
 
-    Per form: the first `serve_plain` requests run one at a time (the plain per-solve GPU
-    throughput), then the whole stream is submitted on its Poisson arrival schedule to a
-    server with `slots` slots (continuous batching: a request starts as soon as a slot and
-    its environments' HBM footprint are free).  speedup_vs_plain = stream solves/s divided by
-    the plain solves/s; the same first requests are also run all at once (speedup on
-    identical requests).  Every energy is checked against the exact free-fermion levels of
-    its chain, and the plain and stream results of the same request must agree."""
+    The plain per-solve GPU throughput is the FP64 form solving the first `serve_plain`
+    requests one at a time.  The serving loop (continuous batching with `slots` slots: a
+    request starts as soon as a slot and its environments' HBM footprint are free) then
+    takes the whole stream on its Poisson arrival schedule, at each rate of `serve_rates`,
+    in the precision form and once in the FP64 form.  speedup_vs_plain = serving solves/s
+    divided by the plain FP64 per-solve throughput; speedup_same_form divides by the same
+    form's one-at-a-time throughput instead (the concurrency gain alone).  Every energy is
+    checked against the exact free-fermion levels of its chain, and a request's energies
+    must be the same alone and in the stream."""
     from nutcracker_b200 import operators
     from nutcracker_b200.serve import Server
 
@@ -239,7 +253,8 @@ def serving_sample(args):
         chi = int(min(rng.integers(16, chi_hi + 1), 2 ** (n // 2)))
         levels = int(rng.integers(1, 5))
         reqs.append((n, lam, chi, levels))
-    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, size=len(reqs)))
+    gaps = rng.exponential(1.0, size=len(reqs))   # unit-rate Poisson gaps, scaled per rate
+    rates = [float(r) for r in args.serve_rates.split(",")]
     ops = {}
 
     def op(n, lam):
@@ -249,39 +264,44 @@ def serving_sample(args):
 
     slots = args.serve_slots or max(1, min(32, 2 * (os.cpu_count() or 4)))
 
-    def one_form(precision):
-        def submit(srv, r, k):
-            n, lam, chi, levels = r
-            return srv.submit(op(n, lam), levels=levels, initial_bandwidth_dimension=chi, seed=1000 + k,
-                              precision=precision)
+    def submit(srv, r, k, precision):
+        n, lam, chi, levels = r
+        return srv.submit(op(n, lam), levels=levels, initial_bandwidth_dimension=chi, seed=1000 + k,
+                          precision=precision)
 
+    def warm(srv, precision):
+        w = operators.ferromagnetic_transverse_ising(16, 1.0)
+        for i in [srv.submit(w, levels=1, initial_bandwidth_dimension=16, seed=1, precision=precision)
+                  for _ in range(slots)]:
+            srv.wait(i)
+
+    def one_at_a_time(precision):
         with Server(max_inflight=slots) as srv:
-            warm = operators.ferromagnetic_transverse_ising(16, 1.0)
-            for i in [srv.submit(warm, levels=1, initial_bandwidth_dimension=16, seed=1, precision=precision)
-                      for _ in range(slots)]:
-                srv.wait(i)
-            plain = []
+            warm(srv, precision)
+            out = []
             t0 = time.perf_counter()
             for k, r in enumerate(reqs[:args.serve_plain]):
-                plain.append(srv.wait(submit(srv, r, k)))
-            t_plain = time.perf_counter() - t0
-            t0 = time.perf_counter()
-            together = [srv.wait(i) for i in [submit(srv, r, k) for k, r in enumerate(reqs[:args.serve_plain])]]
-            t_together = time.perf_counter() - t0
+                out.append(srv.wait(submit(srv, r, k, precision)))
+            log("serving: %d requests one at a time (precision %d): %.1f s" % (len(out), precision, time.perf_counter() - t0))
+            return out, time.perf_counter() - t0
+
+    def stream(precision, rate):
+        arrivals = np.cumsum(gaps / rate)
+        with Server(max_inflight=slots) as srv:
+            warm(srv, precision)
             start = time.perf_counter()
             ids = []
             for k, r in enumerate(reqs):
                 delay = arrivals[k] - (time.perf_counter() - start)
                 if delay > 0:
                     time.sleep(delay)
-                ids.append(submit(srv, r, k))
+                ids.append(submit(srv, r, k, precision))
             res = [srv.wait(i) for i in ids]
             window = time.perf_counter() - start
             after = srv.stats()
+        log("serving: stream of %d at %.0f/s (precision %d): %.1f s" % (len(reqs), rate, precision, window))
         lat = sorted(x["seconds_total"] for x in res if x["status"] == 0)
         pct = (lambda q: lat[min(len(lat) - 1, int(np.ceil(q * len(lat))) - 1)]) if lat else (lambda q: None)
-        same = max((abs(a - b) / max(abs(a), 1e-300) for p, m in list(zip(plain, res)) + list(zip(plain, together))
-                    for a, b in zip(p["energies"], m["energies"])), default=0.0)
         exact_err, exact_err_full_chi = [], []
         for r, x in zip(reqs, res):
             n, lam, chi, levels = r
@@ -290,48 +310,84 @@ def serving_sample(args):
                 exact_err.append(err)
                 if chi >= 2 ** (n // 2):   # the bond dimension represents the chain exactly
                     exact_err_full_chi.append(err)
-        plain_rate = len(plain) / t_plain if t_plain > 0 else None
-        stream_rate = len(lat) / window if window > 0 else None
-        return {
-            "precision": "mixed (3xTF32 sweeps + FP64 refinement)" if precision else "fp64",
-            "requests": len(reqs), "failed": sum(1 for x in res if x["status"] != 0),
-            "solves_per_s": stream_rate, "p50_s": pct(0.5), "p99_s": pct(0.99),
-            "mean_s": float(np.mean(lat)) if lat else None, "window_s": window,
-            "peak_gb_in_flight": after["peak_bytes_in_flight"] / 1e9,
-            "plain_solves_per_s": plain_rate, "plain_requests": len(plain),
-            "plain_mean_s": t_plain / max(1, len(plain)),
-            "speedup_vs_plain": (stream_rate / plain_rate) if (stream_rate and plain_rate) else None,
-            "speedup_same_requests": t_plain / t_together if t_together > 0 else None,
-            "max_rel_diff_alone_vs_mix": same,
+        return res, {
+            "rate_per_s": rate, "requests": len(reqs), "failed": sum(1 for x in res if x["status"] != 0),
+            "solves_per_s": len(lat) / window if window > 0 else None,
+            "p50_s": pct(0.5), "p99_s": pct(0.99), "mean_s": float(np.mean(lat)) if lat else None,
+            "window_s": window, "peak_gb_in_flight": after["peak_bytes_in_flight"] / 1e9,
             "max_dE_per_site_vs_exact": max(exact_err) if exact_err else None,
             "max_dE_per_site_vs_exact_where_chi_is_exact": max(exact_err_full_chi) if exact_err_full_chi else None,
         }
 
+    def same(a_list, b_list):
+        return max((abs(a - b) / max(abs(a), 1e-300) for p, m in zip(a_list, b_list)
+                    for a, b in zip(p["energies"], m["energies"])), default=0.0)
+
+    plain64, t64 = one_at_a_time(0)
+    plain_rate = len(plain64) / t64
     out = {
         "workload": "TFIM -ZZ - lam X: lam~U[0.5,1.5], N~U{8..%d}, chi~U{16..%d} (<= chain maximum), 1-4 levels, "
-                    "Poisson arrivals at %.0f/s; %d requests (bounded sample of the 20k-request stream)"
-                    % (n_hi, chi_hi, args.serve_rate, len(reqs)),
+                    "Poisson arrivals; %d requests (bounded sample of the 20k-request stream)"
+                    % (n_hi, chi_hi, len(reqs)),
         "slots": slots,
-        "speedup_definition": "stream solves/s (all requests on their Poisson schedule) / plain solves/s (the "
-                              "first plain_requests requests one at a time); speedup_same_requests: those "
-                              "requests one at a time vs all at once",
+        "plain": {"form": "fp64", "requests": len(plain64), "solves_per_s": plain_rate, "mean_s": t64 / len(plain64)},
+        "speedup_definition": "serving-loop solves/s over the stream / plain FP64 per-solve throughput (the first "
+                              "plain requests one at a time); speedup_same_form: / the same form's one-at-a-time "
+                              "throughput",
         "exact": "free-fermion levels of every request (truncation error included where chi < 2^(N/2))",
-        "fp64": one_form(0),
     }
-    if not args.serve_no_mixed:
-        out["mixed"] = one_form(1)
+    forms = [("mixed", 1)] if not args.serve_no_mixed else []
+    forms.append(("fp64", 0))
+    for name, prec in forms:
+        if prec:
+            plain_f, t_f = one_at_a_time(prec)
+            rate_f = len(plain_f) / t_f
+        else:
+            plain_f, rate_f = plain64, plain_rate
+        runs = []
+        for rate in (rates if prec or args.serve_no_mixed else rates[-1:]):
+            res, summary = stream(prec, rate)
+            summary["speedup_vs_plain"] = summary["solves_per_s"] / plain_rate if summary["solves_per_s"] else None
+            summary["speedup_same_form"] = summary["solves_per_s"] / rate_f if summary["solves_per_s"] else None
+            summary["max_rel_diff_alone_vs_stream"] = same(plain_f, res)
+            runs.append(summary)
+        out[name] = {"precision": "mixed (3xTF32 sweeps + FP64 refinement)" if prec else "fp64",
+                     "one_at_a_time_solves_per_s": rate_f, "streams": runs,
+                     "max_rel_diff_plain_fp64_vs_form": same(plain64, plain_f)}
+    best = max((r["speedup_vs_plain"] or 0 for f in ("mixed", "fp64") if f in out for r in out[f]["streams"]),
+               default=None)
+    out["speedup_vs_plain_best"] = best
+    return out
+
+
+def guarded_sample(fn, args):
+    """A secondary sample of the bench line; a failure is recorded in its
+    object instead of losing the headline measurement."""
+    t0 = time.perf_counter()
+    try:
+        out = fn(args)
+    except Exception as e:   # noqa: BLE001 - reported in the line
+        out = {"error": "%s: %s" % (type(e).__name__, e)}
+    out["sample_wall_s"] = time.perf_counter() - t0
     return out
 
 
 def batched_sample(args):
     """Batched workload sample: independent XXZ chains H = sum_i J_i (XX + YY + Delta_i ZZ)
     with per-bond J_i ~ U[0.5,1.5], Delta_i ~ U[0,2], N ~ U{8..48}, chi ~ U{8..128} (capped
-    at the chain's maximum bond dimension), ground state in FP64, seeded.  The whole
-    batch is solved one chain at a time (the plain per-chain throughput), then submitted
-    at once to the serving engine, whose workers (each with its own stream and arena)
-    keep many chains in flight on the GPU."""
+    at the chain's maximum bond dimension), ground state, seeded.  The batch goes through
+    the lockstep engine (nc_batch: one persistent grouped launch per contraction stage
+    over every chain, one CUDA-graph replay per Lanczos iteration of every chain,
+    complex64 contractions with FP64 Krylov and an FP64 refinement), timed with CUDA
+    events around nc_batch_solve.  The plain per-chain throughput is the single-chain
+    FP64 engine solving the first `plain` chains of the batch one at a time; the same
+    chains are also solved as a batch of their own, and each of them alone through the
+    batched engine (the energies must be identical alone and in the batch)."""
+    import torch
+
     from nutcracker_b200 import operators
-    from nutcracker_b200.serve import Server
+    from nutcracker_b200.batched import Batch, load_tile_table
+    from nutcracker_b200.chain import Chain
 
     rng = np.random.default_rng(args.seed + 11)
     chains = []
@@ -339,41 +395,64 @@ def batched_sample(args):
         n = int(rng.integers(8, 49))
         chi = int(min(rng.integers(8, 129), 2 ** (n // 2)))
         chains.append((n, operators.xxz_random(n, rng), chi))
-    slots = args.serve_slots or max(1, min(16, os.cpu_count() or 4))
+    seeds = [3000 + k for k in range(len(chains))]
+    table = load_tile_table()
 
-    def submit(srv, k):
+    def run_batch(idx):
+        with Batch([chains[k][1] for k in idx], [chains[k][2] for k in idx], seeds=[seeds[k] for k in idx],
+                   tile_table=table, maximum_sweeps=200) as b:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res = b.solve()
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            st = b.stats()
+        return res, st, dt
+
+    # warm-up (module load, graph instantiation paths)
+    run_batch(list(range(min(4, len(chains)))))
+    res, st, window = run_batch(list(range(len(chains))))
+    log("batched: %d chains in %.1f s" % (len(chains), window))
+    nplain = min(args.batch_plain, len(chains))
+    sub = list(range(nplain))
+    # plain: the single-chain FP64 engine, one chain at a time
+    plain_e = []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in sub:
         n, op, chi = chains[k]
-        return srv.submit(op, levels=1, initial_bandwidth_dimension=chi, seed=3000 + k)
-
-    with Server(max_inflight=slots) as srv:
-        warm = operators.xxz_random(16, np.random.default_rng(1))
-        for i in [srv.submit(warm, levels=1, initial_bandwidth_dimension=16, seed=1) for _ in range(slots)]:
-            srv.wait(i)
-        # every chain of the batch one at a time, then the whole batch at once
-        plain = []
-        t0 = time.perf_counter()
-        for k in range(len(chains)):
-            plain.append(srv.wait(submit(srv, k)))
-        t_plain = time.perf_counter() - t0
-        start = time.perf_counter()
-        ids = [submit(srv, k) for k in range(len(chains))]
-        res = [srv.wait(i) for i in ids]
-        window = time.perf_counter() - start
-    ok = [x for x in res if x["status"] == 0]
-    same = max((abs(p["energies"][0] - m["energies"][0]) / max(abs(p["energies"][0]), 1e-300)
-                for p, m in zip(plain, res)), default=0.0)
-    plain_rate = len(plain) / t_plain if t_plain > 0 else None
-    rate = len(ok) / window if window > 0 else None
+        ch = Chain(op, initial_bandwidth_dimension=chi, seed=seeds[k])
+        plain_e.append(ch.solve_levels_at_bandwidth(1)[0])
+        del ch
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter() - t0
+    log("batched: %d chains one at a time (single-chain engine) in %.1f s" % (nplain, t_plain))
+    res_sub, st_sub, window_sub = run_batch(sub)
+    alone = [run_batch([k])[0][0]["energy"] for k in sub[:4]]
+    same = max(abs(a - res[k]["energy"]) / abs(a) for k, a in zip(sub[:4], alone))
+    dev_plain = max(abs(res[k]["energy"] - e) / chains[k][0] for k, e in zip(sub, plain_e))
+    rate = len(chains) / window
+    plain_rate = nplain / t_plain
     return {
         "workload": "XXZ chains sum J_i (XX + YY + Delta_i ZZ): J_i~U[0.5,1.5], Delta_i~U[0,2] per bond, "
-                    "N~U{8..48}, chi~U{8..128} (<= chain maximum), ground state, FP64; %d chains (bounded "
-                    "sample of the 4096-chain batch)" % len(chains),
-        "slots": slots, "chains": len(chains), "failed": len(chains) - len(ok),
+                    "N~U{8..48}, chi~U{8..128} (<= chain maximum), ground state; %d chains (bounded sample "
+                    "of the 4096-chain batch); complex64 contractions, FP64 Krylov, FP64 refinement "
+                    "sweeps" % len(chains),
+        "engine": "nc_batch lockstep: one grouped launch per contraction stage, Lanczos iteration as "
+                  "one CUDA graph replay",
+        "chains": len(chains), "unconverged": sum(1 for r in res if not r["converged"]),
         "chains_per_s": rate, "window_s": window,
-        "plain_chains_per_s": plain_rate, "plain_chains": len(plain),
-        "speedup_vs_plain": (rate / plain_rate) if (rate and plain_rate) else None,
-        "speedup_definition": "the same chains: one at a time vs all submitted at once",
+        "global_steps": st["global_steps"], "lanczos_iterations": st["lanczos_iterations"],
+        "kernel_launches": st["kernel_launches"], "device_bytes": st["device_bytes"],
+        "mean_sweeps": float(np.mean([r["sweeps"] for r in res])),
+        "tile_table_entries": len(table),
+        "plain_chains": nplain, "plain_chains_per_s": plain_rate,
+        "plain_definition": "single-chain FP64 engine (nc_chain), the first %d chains one at a time" % nplain,
+        "speedup_vs_plain": rate / plain_rate,
+        "same_chains_batched_chains_per_s": nplain / window_sub,
+        "same_chains_speedup": (nplain / window_sub) / plain_rate,
         "max_rel_diff_alone_vs_batch": same,
+        "max_abs_dE_per_site_vs_single_chain_fp64": dev_plain,
     }
 
 
@@ -416,6 +495,7 @@ def config3_spin1_sample(args):
             secs.append(time.perf_counter() - t0)
             energies.append(c.get_energy())
             sweeps.append(c.info()["sweeps"] - s0)
+            log("config3 %s level %d: %.1f s" % (name, k, secs[-1]))
         out[name] = {"energies": energies, "seconds": secs, "sweeps": sweeps}
     e64, emx = out["fp64"]["energies"], out["mixed"]["energies"]
     out["dE_per_site_per_level"] = [abs(a - b) / n for a, b in zip(emx, e64)]
@@ -756,12 +836,14 @@ def run_ours(args, rank, world):
         n, ms, fl = ct.c_uint64(), ct.c_double(), ct.c_double()
         nb.lib.nc_profile_end(ct.byref(n), ct.byref(ms), ct.byref(fl))
 
+    log("start: N=%d chi %d -> %d, %d warm-up + %d timed sweeps per form" % (args.sites, args.chi_start, args.chi, args.warmup, args.steps))
     ops = operators.heisenberg(args.sites)
     chain = Chain(ops, initial_bandwidth_dimension=args.chi_start, seed=replica_seed(args.seed, rank),
                   time_phases=1 if args.phases else 0)
     for _ in range(args.presweeps):
         chain.perform_optimization_sweep()
     chain.increase_bandwidth_dimension(args.chi)
+    log("grown to chi=%d" % args.chi)
     # common start of both forms: the freshly grown chi=1024 state (no sweep
     # at chi=1024 yet), so both timed windows include the transient after
     # the growth and the energy differences are due to precision alone
@@ -781,6 +863,7 @@ def run_ours(args, rank, world):
         chain.set_state(start)
         for _ in range(args.warmup):
             chain.perform_optimization_sweep()
+    log("warm-up done")
     clocks = ClockSampler(local)
     clocks.start()
     res = {}
@@ -800,6 +883,7 @@ def run_ours(args, rank, world):
                        "energy": chain.get_energy(), "info0": info0, "info1": info1}
         chain.perform_optimization_sweep()            # one more FP64 sweep: the reference for the closing sweep
         res["fp64"]["energy_plus1"] = chain.get_energy()
+        log("fp64 timed: %.1f s" % t64)
 
     if wantmx:
         chain.set_precision(1)
@@ -834,6 +918,7 @@ def run_ours(args, rank, world):
         torch.cuda.synchronize()
         res["mixed"]["closing_sweep_s"] = c0.elapsed_time(c1) / 1e3
         res["mixed"]["energy_closed"] = chain.get_energy()
+        log("mixed timed: %.1f s" % tmx)
     clk = clocks.stop()
 
     # e2e through the public API: state from pinned host memory -> sweep -> energy back
@@ -971,12 +1056,16 @@ def run_ours(args, rank, world):
         line.update({"value": line["fp64"]["value"], "ms_per_step": line["fp64"]["ms_per_step"],
                      "dtype": "complex128", "gpu_launches": line["fp64"]["gpu_launches"],
                      "roofline": line["fp64"]["roofline"], "chain": line["fp64"]["chain"]})
+    log("e2e done")
     if world == 1 and not args.no_serving:
-        line["serving"] = serving_sample(args)
+        line["serving"] = guarded_sample(serving_sample, args)
+        log("serving sample: %.1f s" % line["serving"]["sample_wall_s"])
     if world == 1 and not args.no_batched:
-        line["batched"] = batched_sample(args)
+        line["batched"] = guarded_sample(batched_sample, args)
+        log("batched sample: %.1f s" % line["batched"]["sample_wall_s"])
     if world == 1 and not args.no_config3:
-        line["config3_spin1"] = config3_spin1_sample(args)
+        line["config3_spin1"] = guarded_sample(config3_spin1_sample, args)
+        log("config3 sample: %.1f s" % line["config3_spin1"]["sample_wall_s"])
     if world == 1 and not args.no_cpu_baseline:
         validation = None
         if not args.no_cpu_validation:
@@ -987,6 +1076,7 @@ def run_ours(args, rank, world):
             validation = cpu_validation(ops, small.state_sites(), args.cpu_validation_s)
             del small
         line["cpu_baseline"] = cpu_baseline(args.sites, args.chi, validation)
+        log("cpu baseline done")
     print(json.dumps(line), flush=True)
 
 
