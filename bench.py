@@ -112,6 +112,9 @@ def parse():
     ap.add_argument("--batch-plain", type=int, default=16,
                     help="chains of the batch also solved one at a time by the single-chain engine")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--time-budget", type=float, default=900.0,
+                    help="seconds after which the remaining secondary samples (serving, batched, spin-1) are "
+                         "skipped and recorded as such, so that a run ends within minutes")
     ap.add_argument("--no-cpu-validation", action="store_true",
                     help="skip the oracle's measured chi=128 sweep segment that checks the extrapolation model")
     ap.add_argument("--cpu-validation-s", type=float, default=60.0)
@@ -346,6 +349,9 @@ def serving_sample(args):
             plain_f, rate_f = plain64, plain_rate
         runs = []
         for rate in (rates if prec or args.serve_no_mixed else rates[-1:]):
+            if runs and time.perf_counter() - T_START > args.time_budget:
+                runs.append({"rate_per_s": rate, "skipped": "time budget"})
+                continue
             res, summary = stream(prec, rate)
             summary["speedup_vs_plain"] = summary["solves_per_s"] / plain_rate if summary["solves_per_s"] else None
             summary["speedup_same_form"] = summary["solves_per_s"] / rate_f if summary["solves_per_s"] else None
@@ -354,7 +360,7 @@ def serving_sample(args):
         out[name] = {"precision": "mixed (3xTF32 sweeps + FP64 refinement)" if prec else "fp64",
                      "one_at_a_time_solves_per_s": rate_f, "streams": runs,
                      "max_rel_diff_plain_fp64_vs_form": same(plain64, plain_f)}
-    best = max((r["speedup_vs_plain"] or 0 for f in ("mixed", "fp64") if f in out for r in out[f]["streams"]),
+    best = max((r.get("speedup_vs_plain") or 0 for f in ("mixed", "fp64") if f in out for r in out[f]["streams"]),
                default=None)
     out["speedup_vs_plain_best"] = best
     return out
@@ -364,6 +370,9 @@ def guarded_sample(fn, args):
     """A secondary sample of the bench line; a failure is recorded in its
     object instead of losing the headline measurement."""
     t0 = time.perf_counter()
+    if t0 - T_START > args.time_budget:
+        return {"skipped": "the run had used %.0f s of its %.0f s budget before this sample (--time-budget)"
+                % (t0 - T_START, args.time_budget), "sample_wall_s": 0.0}
     try:
         out = fn(args)
     except Exception as e:   # noqa: BLE001 - reported in the line

@@ -547,6 +547,8 @@ typedef struct {
     uint32_t maximum_sweeps;          /* FP64 sweeps per chain, 0 (default): no bound; a chain that
                                          reaches it stops and reports converged = 0 */
     uint64_t seed;                    /* seed of every chain when no per-chain seeds are given */
+    uint32_t time_phases;             /* nonzero: synchronise after the moves and after the solves of
+                                         every global step and time them (diagnostics) */
 } nc_batch_options;
 typedef struct {
     double energy;                    /* the last accepted site energy of the final sweep */
@@ -564,6 +566,9 @@ typedef struct {
     uint64_t kernel_launches;         /* kernels launched, graph nodes included */
     uint64_t device_bytes;            /* the batch's device allocation */
     double seconds;                   /* wall time of the last nc_batch_solve */
+    double seconds_moves, seconds_solves;   /* with time_phases: gauge moves + environments, site solves */
+    uint64_t restart_rounds;          /* Lanczos restarts of the lockstep solver (every chain at once) */
+    uint64_t max_iterations_per_step; /* most Lanczos iterations one global step needed */
 } nc_batch_stats;
 typedef struct nc_batch nc_batch;
 

@@ -1192,7 +1192,8 @@ struct Engine {
 
     // statistics
     uint64_t global_steps = 0, lanczos_iterations = 0, graph_launches = 0, launches = 0;
-    double seconds = 0;
+    uint64_t restart_rounds = 0, max_iterations_per_step = 0;
+    double seconds = 0, seconds_moves = 0, seconds_solves = 0;   // the last two with time_phases
 
     ~Engine() {
         if (graph_exec) cudaGraphExecDestroy(graph_exec);
@@ -1702,12 +1703,14 @@ struct Engine {
         launches += 4;
         const int m_max = (int)opt.krylov_dimension;
         const int check_every = 4;
+        uint64_t iters = 0;
         for (;;) {
             int active = 1;
             for (int it = 0; it < m_max; ++it) {
                 NC_CUDA(cudaGraphLaunch(graph_exec, stream));
                 graph_launches++;
                 lanczos_iterations++;
+                iters++;
                 launches += kGraphKernels;
                 if ((it + 1) % check_every == 0 || it + 1 == m_max) {
                     active = read_active();
@@ -1727,7 +1730,9 @@ struct Engine {
             NC_CHECK_LAUNCH();
             launches++;
             if (read_active() == 0) break;
+            restart_rounds++;
         }
+        max_iterations_per_step = std::max(max_iterations_per_step, iters);
         lz_form_kernel<2><<<grid_vec, kLzT, 0, stream>>>(lz_chunks.d.p, lz_chunks.d_count.p, d_lz.p, st, d_solving.p,
                                                          d_part.p);
         lz_norm_kernel<2><<<tb, 256, 0, stream>>>(B, d_lz.p, st, d_solving.p, d_part.p, sanity);
@@ -1765,8 +1770,20 @@ struct Engine {
             }
             if (solvers.empty()) break;
             global_steps++;
-            do_moves(movers, prec);
-            do_solves(solvers, prec, site_tol, sanity);
+            if (opt.time_phases) {
+                auto t0 = std::chrono::steady_clock::now();
+                do_moves(movers, prec);
+                NC_CUDA(cudaStreamSynchronize(stream));
+                auto t1 = std::chrono::steady_clock::now();
+                do_solves(solvers, prec, site_tol, sanity);
+                NC_CUDA(cudaStreamSynchronize(stream));
+                auto t2 = std::chrono::steady_clock::now();
+                seconds_moves += std::chrono::duration<double>(t1 - t0).count();
+                seconds_solves += std::chrono::duration<double>(t2 - t1).count();
+            } else {
+                do_moves(movers, prec);
+                do_solves(solvers, prec, site_tol, sanity);
+            }
             bool sweep_end = false;
             for (int c : solvers) {
                 ChainHost& ch = chains[c];
@@ -1960,6 +1977,10 @@ int nc_batch_get_stats(nc_batch* b, nc_batch_stats* st) {
     st->graph_launches = b->e.graph_launches;
     st->kernel_launches = b->e.launches;
     st->seconds = b->e.seconds;
+    st->seconds_moves = b->e.seconds_moves;
+    st->seconds_solves = b->e.seconds_solves;
+    st->restart_rounds = b->e.restart_rounds;
+    st->max_iterations_per_step = b->e.max_iterations_per_step;
     st->device_bytes = b->e.pool_bytes;
     NC_ABI_END
     return nc::g_status;

@@ -35,6 +35,7 @@ class nc_batch_options(ct.Structure):
         ("sweep_convergence_threshold", ct.c_double),
         ("maximum_sweeps", ct.c_uint32),
         ("seed", ct.c_uint64),
+        ("time_phases", ct.c_uint32),
     ]
 
 
@@ -53,6 +54,8 @@ class nc_batch_stats(ct.Structure):
         ("global_steps", ct.c_uint64), ("lanczos_iterations", ct.c_uint64),
         ("graph_launches", ct.c_uint64), ("kernel_launches", ct.c_uint64),
         ("device_bytes", ct.c_uint64), ("seconds", ct.c_double),
+        ("seconds_moves", ct.c_double), ("seconds_solves", ct.c_double),
+        ("restart_rounds", ct.c_uint64), ("max_iterations_per_step", ct.c_uint64),
     ]
 
 

@@ -38,15 +38,28 @@ def test_tile_table_rejects_unknown_configuration(tmp_path):
 
 
 def test_batch_argument_checks_before_any_device_work():
+    """Runs on a thread of its own: the library's error status is per host
+    thread, and the failing calls here must not leave it set for later tests."""
+    import threading
+
     from nutcracker_b200 import NutcrackerError
     from nutcracker_b200.batched import Batch
 
     ops = mpo.xxz_random(6, np.random.default_rng(0))
-    with pytest.raises(NutcrackerError) as e:
-        Batch([ops], [4], krylov_dimension=30)
-    assert e.value.code == 1002
-    with pytest.raises(NutcrackerError) as e:
-        Batch([ops], [4], precision=2)
-    assert e.value.code == 1002
-    with pytest.raises(ValueError):
-        Batch([ops], [4, 8])
+    seen = {}
+
+    def body():
+        for key, kw in (("krylov", {"krylov_dimension": 30}), ("precision", {"precision": 2})):
+            try:
+                Batch([ops], [4], **kw)
+            except NutcrackerError as e:
+                seen[key] = e.code
+        try:
+            Batch([ops], [4, 8])
+        except ValueError:
+            seen["count"] = True
+
+    t = threading.Thread(target=body)
+    t.start()
+    t.join()
+    assert seen == {"krylov": 1002, "precision": 1002, "count": True}
