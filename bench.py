@@ -89,16 +89,16 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-loop sample")
     ap.add_argument("--serving-only", action="store_true", help="run only the serving-loop sample")
-    ap.add_argument("--serve-requests", type=int, default=48,
+    ap.add_argument("--serve-requests", type=int, default=24,
                     help="requests in the serving sample (the serving workload has 20k; a bounded sample)")
     ap.add_argument("--serve-half", action="store_true",
                     help="halve the serving workload's N and chi ranges (N<=64, chi<=128)")
     ap.add_argument("--serve-no-mixed", action="store_true", help="serve the FP64 form only")
-    ap.add_argument("--serve-plain", type=int, default=12,
+    ap.add_argument("--serve-plain", type=int, default=6,
                     help="requests of the stream timed one at a time and then all at once (the plain "
                          "per-solve baseline and the concurrency speed-up on the same requests)")
     ap.add_argument("--serve-slots", type=int, default=0, help="concurrent requests (0: min(32, 2 x cores))")
-    ap.add_argument("--serve-rates", default="4,64",
+    ap.add_argument("--serve-rates", default="64",
                     help="Poisson arrival rates swept by the serving sample, requests/s (comma-separated)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-form sample")
     ap.add_argument("--no-config3", action="store_true", help="skip the spin-1 precision-form sample")
@@ -112,6 +112,8 @@ def parse():
     ap.add_argument("--batch-plain", type=int, default=16,
                     help="chains of the batch also solved one at a time by the single-chain engine")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-time-to-accuracy", action="store_true",
+                    help="skip the untimed evaluations behind the time-to-accuracy comparison")
     ap.add_argument("--time-budget", type=float, default=900.0,
                     help="seconds after which the remaining secondary samples (serving, batched, spin-1) are "
                          "skipped and recorded as such, so that a run ends within minutes")
@@ -342,6 +344,9 @@ def serving_sample(args):
     forms = [("mixed", 1)] if not args.serve_no_mixed else []
     forms.append(("fp64", 0))
     for name, prec in forms:
+        if out.get("mixed") and time.perf_counter() - T_START > args.time_budget:
+            out[name] = {"skipped": "time budget"}
+            continue
         if prec:
             plain_f, t_f = one_at_a_time(prec)
             rate_f = len(plain_f) / t_f
@@ -360,7 +365,8 @@ def serving_sample(args):
         out[name] = {"precision": "mixed (3xTF32 sweeps + FP64 refinement)" if prec else "fp64",
                      "one_at_a_time_solves_per_s": rate_f, "streams": runs,
                      "max_rel_diff_plain_fp64_vs_form": same(plain64, plain_f)}
-    best = max((r.get("speedup_vs_plain") or 0 for f in ("mixed", "fp64") if f in out for r in out[f]["streams"]),
+    best = max((r.get("speedup_vs_plain") or 0 for f in ("mixed", "fp64") if f in out
+                for r in out[f].get("streams", [])),
                default=None)
     out["speedup_vs_plain_best"] = best
     return out
@@ -789,6 +795,50 @@ def replica_throughput(steps, world, seconds_max):
     return steps * world / seconds_max
 
 
+def time_to_accuracy(args, ops, chain, start, res):
+    """Device time each form needs, from the same freshly grown state, until its
+    energy of record is within 1e-9 per site of the FP64 converged energy (the
+    FP64 form's energy after K+1 sweeps).  FP64: the timed per-sweep device
+    times up to the first sweep whose energy qualifies.  Precision form: the
+    timed per-sweep device times of its mixed sweeps up to the first sweep count
+    k whose FP64 evaluation qualifies, plus the timed FP64 evaluation.  The
+    evaluations are made untimed on a second chain from a copy of the state
+    after k mixed sweeps (k = 1, 2, 3, 4, 6, 8, 12, 16, 20 until one qualifies,
+    so the precision form's time is an upper bound)."""
+    from nutcracker_b200.chain import Chain
+
+    n = args.sites
+    e_ref = res["fp64"]["energy_plus1"]
+    tol = 1e-9 * n
+    per64, en64 = res["fp64"]["per_sweep_s"], res["fp64"]["energies"]
+    k64 = next((k + 1 for k, e in enumerate(en64) if abs(e - e_ref) <= tol), None)
+    out = {"reference_energy": e_ref, "target_dE_per_site": 1e-9,
+           "fp64_sweeps": k64, "fp64_s": sum(per64[:k64]) if k64 else None}
+    permx = res["mixed"]["per_sweep_s"]
+    checkpoints = [k for k in (1, 2, 3, 4, 6, 8, 12, 16, 20) if k <= len(permx)]
+    chain.set_precision(1)
+    chain.set_state(start)
+    ev = Chain(ops, initial_bandwidth_dimension=args.chi, seed=args.seed + 99)
+    evals = []
+    done = 0
+    for k in checkpoints:
+        while done < k:
+            chain.perform_optimization_sweep()
+            done += 1
+        ev.set_state(chain.state_sites())
+        e = ev.get_energy()
+        evals.append({"mixed_sweeps": k, "fp64_evaluation": e, "dE_per_site": abs(e - e_ref) / n})
+        if abs(e - e_ref) <= tol:
+            break
+    del ev
+    kmx = next((x["mixed_sweeps"] for x in evals if x["dE_per_site"] * n <= tol), None)
+    out.update({"mixed_evaluations": evals, "mixed_sweeps": kmx,
+                "mixed_s": (sum(permx[:kmx]) + res["mixed"]["eval_s"]) if kmx else None})
+    if out["fp64_s"] and out["mixed_s"]:
+        out["speedup"] = out["fp64_s"] / out["mixed_s"]
+    return out
+
+
 def run_ours(args, rank, world):
     import ctypes as ct
     import torch
@@ -928,6 +978,9 @@ def run_ours(args, rank, world):
         res["mixed"]["closing_sweep_s"] = c0.elapsed_time(c1) / 1e3
         res["mixed"]["energy_closed"] = chain.get_energy()
         log("mixed timed: %.1f s" % tmx)
+    if want64 and wantmx and not args.no_time_to_accuracy:
+        res["time_to_accuracy"] = time_to_accuracy(args, ops, chain, start, res)
+        log("time to accuracy done")
     clk = clocks.stop()
 
     # e2e through the public API: state from pinned host memory -> sweep -> energy back
@@ -1060,21 +1113,23 @@ def run_ours(args, rank, world):
                         "speedup_definition": "same K sweeps from the same freshly grown state: FP64 sweep time "
                                               "over precision-form sweep time including its FP64 final energy "
                                               "evaluation"})
+        if "time_to_accuracy" in res:
+            acc["time_to_accuracy"] = res["time_to_accuracy"]
         line["accuracy"] = acc
     else:
         line.update({"value": line["fp64"]["value"], "ms_per_step": line["fp64"]["ms_per_step"],
                      "dtype": "complex128", "gpu_launches": line["fp64"]["gpu_launches"],
                      "roofline": line["fp64"]["roofline"], "chain": line["fp64"]["chain"]})
     log("e2e done")
-    if world == 1 and not args.no_serving:
-        line["serving"] = guarded_sample(serving_sample, args)
-        log("serving sample: %.1f s" % line["serving"]["sample_wall_s"])
-    if world == 1 and not args.no_batched:
-        line["batched"] = guarded_sample(batched_sample, args)
-        log("batched sample: %.1f s" % line["batched"]["sample_wall_s"])
     if world == 1 and not args.no_config3:
         line["config3_spin1"] = guarded_sample(config3_spin1_sample, args)
         log("config3 sample: %.1f s" % line["config3_spin1"]["sample_wall_s"])
+    if world == 1 and not args.no_batched:
+        line["batched"] = guarded_sample(batched_sample, args)
+        log("batched sample: %.1f s" % line["batched"]["sample_wall_s"])
+    if world == 1 and not args.no_serving:
+        line["serving"] = guarded_sample(serving_sample, args)
+        log("serving sample: %.1f s" % line["serving"]["sample_wall_s"])
     if world == 1 and not args.no_cpu_baseline:
         validation = None
         if not args.no_cpu_validation:

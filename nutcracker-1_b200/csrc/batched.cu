@@ -47,6 +47,7 @@
 #include "batched_kernels.cuh"
 #include "nc_abi_util.h"
 #include "nc_common.cuh"
+#include "nc_ritz.cuh"
 #include "nutcracker_b200.h"
 
 namespace nc {
@@ -56,14 +57,18 @@ namespace {
 // ---------------------------------------------------------------------------
 // Per-chain Lanczos state (read by every stage: a finished chain is skipped)
 // ---------------------------------------------------------------------------
+constexpr int kKeepMax = 8;   // Ritz vectors kept by a thick restart
+
 struct LzChain {
     cplx* V;      // (kMaxKrylov + 1) vectors of length n
     cplx* w;      // residual / scratch vector
     cplx* x;      // the site: initial guess, and the result when accepted
+    cplx* Y;      // (kKeepMax + 1) vectors: the kept Ritz vectors and the residual at a restart
     long long n;
     double tol;
     int cstart, ccount;   // the chain's chunks in the chunk list
-    int m_max;            // basis size before an explicit restart
+    int m_max;            // basis size before a thick restart
+    int keep;             // Ritz vectors kept by a restart
     int maxit;            // restarts before the solve fails
 };
 
@@ -73,10 +78,17 @@ struct LzState {
     int stall;      // 1: basis full, waiting for a restart
     int adv;        // 1: the next basis vector is to be written
     int restarts, matvecs, fail, accept;
-    double alpha[kMaxKrylov], beta[kMaxKrylov], s[kMaxKrylov];
-    double theta, res, xnorm, energy;
+    double theta, res, beta, tnorm, xnorm, energy;
     cplx h1[kMaxKrylov + 1], h2[kMaxKrylov + 1];
     double wn2;
+};
+
+// The projected problem of one chain (nc_ritz.cuh): its kept decomposition,
+// the ordered Ritz vectors S (column r at S[kMaxKrylov * r]) and values.
+struct LzRitz {
+    double state[2 * kMaxKrylov * kMaxKrylov];
+    double S[kMaxKrylov * kMaxKrylov];
+    double theta[kMaxKrylov];
 };
 
 // ---------------------------------------------------------------------------
@@ -462,84 +474,36 @@ __global__ void lz_reduce_kernel(int nchains, const LzChain* __restrict__ ch, Lz
     else S.wn2 = x;
 }
 
-// Lowest eigenpair of the symmetric tridiagonal T (diagonal a[0..k), off-
-// diagonal b[0..k-1)): the eigenvalue by Sturm-sequence bisection, the
-// eigenvector by inverse iteration with the shift just below it (T - sigma I
-// positive definite, LDL^T without pivoting).
-__device__ void tridiag_lowest(int k, const double* a, const double* b, double* theta_out, double* s) {
-    double lo = a[0], hi = a[0];
-    for (int i = 0; i < k; ++i) {
-        const double r = (i > 0 ? fabs(b[i - 1]) : 0.0) + (i + 1 < k ? fabs(b[i]) : 0.0);
-        lo = fmin(lo, a[i] - r);
-        hi = fmax(hi, a[i] + r);
-    }
-    const double scale = fmax(fabs(lo), fabs(hi)) + 1e-300;
-    // count of eigenvalues < x
-    auto count = [&](double x) {
-        int neg = 0;
-        double q = a[0] - x;
-        if (q < 0) ++neg;
-        for (int i = 1; i < k; ++i) {
-            const double qq = (fabs(q) < 1e-300 * scale) ? copysign(1e-300 * scale, q) : q;
-            q = (a[i] - x) - b[i - 1] * b[i - 1] / qq;
-            if (q < 0) ++neg;
-        }
-        return neg;
-    };
-    for (int it = 0; it < 200 && hi - lo > 2.2e-16 * scale; ++it) {
-        const double mid = 0.5 * (lo + hi);
-        if (mid <= lo || mid >= hi) break;
-        if (count(mid) >= 1) hi = mid;
-        else lo = mid;
-    }
-    const double theta = hi;
-    // inverse iteration: (T - sigma I) s_new = s, sigma = theta - delta
-    const double sigma = theta - 64.0 * 2.2e-16 * scale;
-    double dd[kMaxKrylov], ll[kMaxKrylov];
-    dd[0] = a[0] - sigma;
-    for (int i = 1; i < k; ++i) {
-        ll[i] = b[i - 1] / dd[i - 1];
-        dd[i] = (a[i] - sigma) - ll[i] * b[i - 1];
-        if (!(dd[i] > 0)) dd[i] = 1e-300 * scale;
-    }
-    if (!(dd[0] > 0)) dd[0] = 1e-300 * scale;
-    for (int i = 0; i < k; ++i) s[i] = 1.0 / sqrt((double)k) * (1.0 + 1e-3 * i);
-    for (int rep = 0; rep < 3; ++rep) {
-        // L y = s
-        for (int i = 1; i < k; ++i) s[i] -= ll[i] * s[i - 1];
-        // D z = y
-        for (int i = 0; i < k; ++i) s[i] /= dd[i];
-        // L^T x = z
-        for (int i = k - 2; i >= 0; --i) s[i] -= ll[i + 1] * s[i + 1];
-        double nrm = 0;
-        for (int i = 0; i < k; ++i) nrm += s[i] * s[i];
-        nrm = 1.0 / sqrt(nrm);
-        for (int i = 0; i < k; ++i) s[i] *= nrm;
-    }
-    *theta_out = theta;
-}
-
-// Per chain: alpha_j, beta_j, the Ritz problem and the decision.
-__global__ void lz_step_kernel(int nchains, const LzChain* __restrict__ ch, LzState* __restrict__ st,
-                               int* __restrict__ active) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c == 0) *active = 0;
+// One warp per chain: column j of the projected matrix from the
+// reorthogonalisation coefficients, the Ritz pairs (warm-started Jacobi,
+// nc_ritz.cuh), and the decision: converged (ARPACK's rule, Ritz estimate
+// <= tol * max(|theta|, eps^(2/3)), or the Krylov space exhausted or
+// invariant), basis full (thick restart), or advance.
+__global__ void __launch_bounds__(32) lz_ritz_kernel(int nchains, const LzChain* __restrict__ ch,
+                                                     LzState* __restrict__ st, LzRitz* __restrict__ rz,
+                                                     int* __restrict__ active) {
+    __shared__ RitzSmem<kMaxKrylov> w;
+    const int c = blockIdx.x;
+    if (c == 0 && threadIdx.x == 0) *active = 0;
     if (c >= nchains) return;
     LzState& S = st[c];
     if (S.done || S.stall) return;
     const LzChain C = ch[c];
     const int j = S.j;
-    S.alpha[j] = S.h1[j].x + S.h2[j].x;
-    S.beta[j] = sqrt(fmax(S.wn2, 0.0));
+    LzRitz& R = rz[c];
+    const RitzResult r =
+        ritz_update_warp<kMaxKrylov, false>(w, j + 1, R.state, S.h1, S.h2, fmax(S.wn2, 0.0), RITZ_SR, R.S,
+                                            kMaxKrylov, R.theta);
+    if (threadIdx.x != 0) return;
     S.matvecs++;
-    double theta, s[kMaxKrylov];
-    tridiag_lowest(j + 1, S.alpha, S.beta, &theta, s);
-    for (int i = 0; i <= j; ++i) S.s[i] = s[i];
-    S.theta = theta;
-    S.res = S.beta[j] * fabs(s[j]);
-    const double eps23 = 3.666852862501036e-11;   // (2^-52)^(2/3), ARPACK's floor
-    const double anorm = fmax(fabs(theta), eps23);
-    if (S.res <= C.tol * anorm || (long long)(j + 1) >= C.n) {
+    S.theta = r.theta;
+    S.res = r.res;
+    S.beta = r.beta;
+    S.tnorm = r.tnorm;
+    const double eps = 2.220446049250313e-16;
+    const double eps23 = 3.666852862501036e-11;   // eps^(2/3), ARPACK's floor
+    const double anorm = fmax(fabs(r.theta), eps23);
+    if (r.res <= C.tol * anorm || (long long)(j + 1) >= C.n || r.beta <= 1e3 * eps * fmax(r.tnorm, 1e-300)) {
         S.done = 1;
     } else if (j + 1 >= C.m_max) {
         S.stall = 1;
@@ -557,7 +521,7 @@ __global__ void __launch_bounds__(kLzT) lz_next_kernel(const VChunk* __restrict_
         const LzState& S = st[c.chain];
         if (!S.adv) continue;
         const LzChain C = ch[c.chain];
-        const double f = 1.0 / S.beta[S.j];
+        const double f = 1.0 / S.beta;
         cplx* vn = C.V + (long long)(S.j + 1) * C.n;
         for (int i = c.off + threadIdx.x; i < c.off + c.len; i += kLzT) vn[i] = cscale(C.w[i], f);
     }
@@ -592,27 +556,24 @@ __global__ void lz_init_kernel(int nchains, const int* __restrict__ solving, LzS
 }
 
 // MODE 0: V_0 = x (the guess), part = |x|^2   (chains with !done)
-// MODE 1: w = sum_k s_k V_k (Ritz vector), part = |w|^2   (chains with stall)
-// MODE 2: w = sum_k s_k V_k, part = |w|^2   (chains with done && !fail, solving)
+// MODE 2: w = V S(:,0) (the wanted Ritz vector), part = |w|^2   (chains with done && !fail, solving)
 template <int MODE>
 __global__ void __launch_bounds__(kLzT) lz_form_kernel(const VChunk* __restrict__ chunks, const int* __restrict__ nchunks,
                                                        const LzChain* __restrict__ ch, const LzState* __restrict__ st,
-                                                       const int* __restrict__ solving, cplx* __restrict__ part) {
+                                                       const LzRitz* __restrict__ rz, const int* __restrict__ solving,
+                                                       cplx* __restrict__ part) {
     __shared__ cplx red[kLzW * (kMaxKrylov + 1)];
     __shared__ double ss[kMaxKrylov];
     const int total = *nchunks;
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
         const VChunk c = chunks[t];
         const LzState& S = st[c.chain];
-        bool on;
-        if (MODE == 0) on = !S.done;
-        else if (MODE == 1) on = !S.done && S.stall;
-        else on = solving[c.chain] && S.done && !S.fail;
+        const bool on = (MODE == 0) ? !S.done : (solving[c.chain] && S.done && !S.fail);
         if (!on) continue;
         const LzChain C = ch[c.chain];
         const int nk = S.j + 1;
         __syncthreads();
-        if (MODE > 0 && threadIdx.x < nk) ss[threadIdx.x] = S.s[threadIdx.x];
+        if (MODE > 0 && threadIdx.x < nk) ss[threadIdx.x] = rz[c.chain].S[threadIdx.x];
         __syncthreads();
         double ar[1] = {0}, ai[1] = {0};
         for (int i = c.off + threadIdx.x; i < c.off + c.len; i += kLzT) {
@@ -638,7 +599,6 @@ __global__ void __launch_bounds__(kLzT) lz_form_kernel(const VChunk* __restrict_
 
 // Per chain, after lz_form_kernel<MODE>: the norm of the formed vector.
 //   MODE 0: xnorm (a vanishing guess fails the solve)
-//   MODE 1: restart bookkeeping (or failure after maxit restarts)
 //   MODE 2: acceptance rule (base_chain.cpp:97-103) and the energy
 template <int MODE>
 __global__ void lz_norm_kernel(int nchains, const LzChain* __restrict__ ch, LzState* __restrict__ st,
@@ -646,10 +606,7 @@ __global__ void lz_norm_kernel(int nchains, const LzChain* __restrict__ ch, LzSt
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nchains) return;
     LzState& S = st[c];
-    bool on;
-    if (MODE == 0) on = !S.done;
-    else if (MODE == 1) on = !S.done && S.stall;
-    else on = solving[c] && S.done && !S.fail;
+    const bool on = (MODE == 0) ? !S.done : (solving[c] && S.done && !S.fail);
     if (!on) return;
     const LzChain C = ch[c];
     double x = 0;
@@ -661,15 +618,6 @@ __global__ void lz_norm_kernel(int nchains, const LzChain* __restrict__ ch, LzSt
             S.done = 1;
             S.fail = 1;
         }
-    } else if (MODE == 1) {
-        if (S.restarts + 1 >= C.maxit || !(nrm > 1e-280)) {
-            S.done = 1;
-            S.fail = 1;
-            S.stall = 0;
-        } else {
-            S.restarts++;
-            S.adv = 2;   // lz_restart_copy_kernel writes V_0
-        }
     } else {
         const double e0 = S.energy, ev = S.theta;
         const double aa = fabs(e0), bb = fabs(ev);
@@ -679,7 +627,7 @@ __global__ void lz_norm_kernel(int nchains, const LzChain* __restrict__ ch, LzSt
     }
 }
 
-// V_0 = w / |w| after a restart (adv == 2); x = w / |w| for an accepted result.
+// MODE 0: V_0 /= |V_0|;  MODE 2: x = w / |w| for an accepted result.
 template <int MODE>
 __global__ void __launch_bounds__(kLzT) lz_scale_kernel(const VChunk* __restrict__ chunks, const int* __restrict__ nchunks,
                                                         const LzChain* __restrict__ ch, const LzState* __restrict__ st,
@@ -689,14 +637,10 @@ __global__ void __launch_bounds__(kLzT) lz_scale_kernel(const VChunk* __restrict
         const VChunk c = chunks[t];
         const LzState& S = st[c.chain];
         const LzChain C = ch[c.chain];
-        if (MODE == 0) {   // normalise the initial basis vector
+        if (MODE == 0) {
             if (S.done) continue;
             const double f = 1.0 / S.xnorm;
             for (int i = c.off + threadIdx.x; i < c.off + c.len; i += kLzT) C.V[i] = cscale(C.V[i], f);
-        } else if (MODE == 1) {
-            if (S.adv != 2) continue;
-            const double f = 1.0 / S.xnorm;
-            for (int i = c.off + threadIdx.x; i < c.off + c.len; i += kLzT) C.V[i] = cscale(C.w[i], f);
         } else {
             if (!(solving[c.chain] && S.accept)) continue;
             const double f = 1.0 / S.xnorm;
@@ -705,13 +649,80 @@ __global__ void __launch_bounds__(kLzT) lz_scale_kernel(const VChunk* __restrict
     }
 }
 
-__global__ void lz_restarted_kernel(int nchains, LzState* __restrict__ st) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+// ---- thick restart (Wu & Simon 2000), for the chains whose basis is full ---
+// Y_i = V S(:,i) for the `keep` wanted Ritz vectors, Y_keep = w / beta (the
+// residual direction, orthogonal to them).
+__global__ void __launch_bounds__(kLzT) lz_restart_form_kernel(const VChunk* __restrict__ chunks,
+                                                               const int* __restrict__ nchunks,
+                                                               const LzChain* __restrict__ ch,
+                                                               const LzState* __restrict__ st,
+                                                               const LzRitz* __restrict__ rz) {
+    __shared__ double ss[kKeepMax * kMaxKrylov];
+    const int total = *nchunks;
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const VChunk c = chunks[t];
+        const LzState& S = st[c.chain];
+        if (S.done || !S.stall) continue;
+        const LzChain C = ch[c.chain];
+        const int m = S.j + 1;
+        __syncthreads();
+        for (int e = threadIdx.x; e < C.keep * kMaxKrylov; e += kLzT) ss[e] = rz[c.chain].S[e];
+        __syncthreads();
+        const double fb = 1.0 / S.beta;
+        for (int i = c.off + threadIdx.x; i < c.off + c.len; i += kLzT) {
+            for (int q = 0; q < C.keep; ++q) {
+                double vr = 0, vi = 0;
+                for (int k = 0; k < m; ++k) {
+                    const cplx b = C.V[(long long)k * C.n + i];
+                    const double f = ss[q * kMaxKrylov + k];
+                    vr = fma(f, b.x, vr);
+                    vi = fma(f, b.y, vi);
+                }
+                C.Y[(long long)q * C.n + i] = cmake(vr, vi);
+            }
+            C.Y[(long long)C.keep * C.n + i] = cscale(C.w[i], fb);
+        }
+    }
+}
+
+// V_0..V_keep = Y_0..Y_keep.
+__global__ void __launch_bounds__(kLzT) lz_restart_copy_kernel(const VChunk* __restrict__ chunks,
+                                                               const int* __restrict__ nchunks,
+                                                               const LzChain* __restrict__ ch,
+                                                               const LzState* __restrict__ st) {
+    const int total = *nchunks;
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const VChunk c = chunks[t];
+        const LzState& S = st[c.chain];
+        if (S.done || !S.stall) continue;
+        const LzChain C = ch[c.chain];
+        for (int q = 0; q <= C.keep; ++q)
+            for (int i = c.off + threadIdx.x; i < c.off + c.len; i += kLzT)
+                C.V[(long long)q * C.n + i] = C.Y[(long long)q * C.n + i];
+    }
+}
+
+// Per chain (one block): the projected matrix becomes diag(theta_0 ..
+// theta_{keep-1}) and the expansion continues from V_keep; after maxit
+// restarts the solve fails (info -14 of the reference, core.f95:2565-2607).
+__global__ void lz_restart_state_kernel(int nchains, const LzChain* __restrict__ ch, LzState* __restrict__ st,
+                                        LzRitz* __restrict__ rz) {
+    const int c = blockIdx.x;
     if (c >= nchains) return;
     LzState& S = st[c];
-    if (S.adv == 2) {
-        S.adv = 0;
-        S.j = 0;
+    if (S.done || !S.stall) return;
+    const LzChain C = ch[c];
+    const bool fail = S.restarts + 1 >= C.maxit;
+    if (!fail) ritz_restart_state<kMaxKrylov>(C.keep, rz[c].theta, rz[c].state);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (fail) {
+            S.done = 1;
+            S.fail = 1;
+        } else {
+            S.restarts++;
+            S.j = C.keep;
+        }
         S.stall = 0;
     }
 }
@@ -1138,7 +1149,7 @@ struct ChainHost {
     std::vector<int> phys, bonds;
     std::vector<MpoDev> ops;
     std::vector<cplx*> site, L, R;
-    cplx *spare = nullptr, *T = nullptr, *U = nullptr, *V = nullptr, *w = nullptr;
+    cplx *spare = nullptr, *T = nullptr, *U = nullptr, *V = nullptr, *w = nullptr, *Y = nullptr;
     cplx *X = nullptr, *Q = nullptr, *tau = nullptr, *rbuf = nullptr;
     size_t max_site = 0;
     // sweep state
@@ -1172,6 +1183,7 @@ struct Engine {
     ChunkList lz_chunks, nrm_chunks;
     DevArray<LzChain> d_lz;
     DevArray<LzState> d_st;
+    DevArray<LzRitz> d_rz;
     DevArray<int> d_solving, d_active;
     DevArray<cplx> d_part, d_part_n;
     DevArray<NormJob> d_norm_jobs;
@@ -1269,6 +1281,7 @@ struct Engine {
                      + env                                                // environments
                      + align_up(mt) + align_up(mu)                        // T, U
                      + (size_t)(kMaxKrylov + 2) * align_up(ms)            // V, w
+                     + (size_t)(kKeepMax + 1) * align_up(ms)              // Y (thick restart)
                      + 2 * align_up(ms) + align_up(mb) + align_up(mb * mb);   // X, Q, tau, R
         }
         pool_bytes = total * sizeof(cplx) + mpo_bytes + 4096;
@@ -1316,6 +1329,7 @@ struct Engine {
             ch.U = take(mu);
             ch.V = take((size_t)(kMaxKrylov + 1) * align_up(ch.max_site));
             ch.w = take(ch.max_site);
+            ch.Y = take((size_t)(kKeepMax + 1) * align_up(ch.max_site));
             ch.X = take(ch.max_site);
             ch.Q = take(ch.max_site);
             ch.tau = take(mb);
@@ -1352,6 +1366,7 @@ struct Engine {
         nrm_chunks.reserve(nchunk_cap);
         d_lz.reserve(B);
         d_st.reserve(B);
+        d_rz.reserve(B);
         d_solving.reserve(B);
         d_active.reserve(1);
         d_part.reserve(nchunk_cap * kPartStride);
@@ -1635,7 +1650,7 @@ struct Engine {
         lz_reduce_kernel<1><<<cb, 256, 0, stream>>>(B, d_lz.p, st, d_part.p);
         lz_cgs_kernel<2><<<grid_vec, kLzT, 0, stream>>>(lz_chunks.d.p, lz_chunks.d_count.p, d_lz.p, st, d_part.p);
         lz_reduce_kernel<2><<<cb, 256, 0, stream>>>(B, d_lz.p, st, d_part.p);
-        lz_step_kernel<<<tb, 256, 0, stream>>>(B, d_lz.p, st, d_active.p);
+        lz_ritz_kernel<<<B, 32, 0, stream>>>(B, d_lz.p, st, d_rz.p, d_active.p);
         lz_next_kernel<<<grid_vec, kLzT, 0, stream>>>(lz_chunks.d.p, lz_chunks.d_count.p, d_lz.p, st);
         lz_inc_kernel<<<tb, 256, 0, stream>>>(B, st, d_active.p);
         cudaError_t e = cudaStreamEndCapture(stream, &graph);
@@ -1684,6 +1699,8 @@ struct Engine {
             z.V = ch.V; z.w = ch.w; z.x = ch.site[i]; z.n = n; z.tol = site_tol;
             z.cstart = r.first; z.ccount = r.second;
             z.m_max = (int)opt.krylov_dimension;
+            z.keep = std::max(1, std::min(std::max(4, z.m_max / 3), z.m_max - 2));
+            z.Y = ch.Y;
             z.maxit = (int)std::max<uint32_t>(1, opt.maximum_number_of_iterations);
             h_solving[c] = 1;
         }
@@ -1696,7 +1713,8 @@ struct Engine {
         capture_graph();
         LzState* st = d_st.p;
         lz_init_kernel<<<tb, 256, 0, stream>>>(B, d_solving.p, st);
-        lz_form_kernel<0><<<grid_vec, kLzT, 0, stream>>>(lz_chunks.d.p, lz_chunks.d_count.p, d_lz.p, st, d_solving.p, d_part.p);
+        lz_form_kernel<0><<<grid_vec, kLzT, 0, stream>>>(lz_chunks.d.p, lz_chunks.d_count.p, d_lz.p, st, d_rz.p, d_solving.p,
+                                                         d_part.p);
         lz_norm_kernel<0><<<tb, 256, 0, stream>>>(B, d_lz.p, st, d_solving.p, d_part.p, sanity);
         lz_scale_kernel<0><<<grid_vec, kLzT, 0, stream>>>(lz_chunks.d.p, lz_chunks.d_count.p, d_lz.p, st, d_solving.p);
         NC_CHECK_LAUNCH();
@@ -1718,13 +1736,12 @@ struct Engine {
                 }
             }
             // chains whose basis is full restart from their Ritz vector
-            lz_form_kernel<1><<<grid_vec, kLzT, 0, stream>>>(lz_chunks.d.p, lz_chunks.d_count.p, d_lz.p, st, d_solving.p,
-                                                             d_part.p);
-            lz_norm_kernel<1><<<tb, 256, 0, stream>>>(B, d_lz.p, st, d_solving.p, d_part.p, sanity);
-            lz_scale_kernel<1><<<grid_vec, kLzT, 0, stream>>>(lz_chunks.d.p, lz_chunks.d_count.p, d_lz.p, st, d_solving.p);
-            lz_restarted_kernel<<<tb, 256, 0, stream>>>(B, st);
+            // thick restart of the chains whose basis is full (the others are skipped)
+            lz_restart_form_kernel<<<grid_vec, kLzT, 0, stream>>>(lz_chunks.d.p, lz_chunks.d_count.p, d_lz.p, st, d_rz.p);
+            lz_restart_copy_kernel<<<grid_vec, kLzT, 0, stream>>>(lz_chunks.d.p, lz_chunks.d_count.p, d_lz.p, st);
+            lz_restart_state_kernel<<<B, 32, 0, stream>>>(B, d_lz.p, st, d_rz.p);
             NC_CHECK_LAUNCH();
-            launches += 4;
+            launches += 3;
             // anything left to iterate?
             count_kernel<<<1, 256, 0, stream>>>(B, st, d_active.p);
             NC_CHECK_LAUNCH();
@@ -1733,7 +1750,7 @@ struct Engine {
             restart_rounds++;
         }
         max_iterations_per_step = std::max(max_iterations_per_step, iters);
-        lz_form_kernel<2><<<grid_vec, kLzT, 0, stream>>>(lz_chunks.d.p, lz_chunks.d_count.p, d_lz.p, st, d_solving.p,
+        lz_form_kernel<2><<<grid_vec, kLzT, 0, stream>>>(lz_chunks.d.p, lz_chunks.d_count.p, d_lz.p, st, d_rz.p, d_solving.p,
                                                          d_part.p);
         lz_norm_kernel<2><<<tb, 256, 0, stream>>>(B, d_lz.p, st, d_solving.p, d_part.p, sanity);
         lz_scale_kernel<2><<<grid_vec, kLzT, 0, stream>>>(lz_chunks.d.p, lz_chunks.d_count.p, d_lz.p, st, d_solving.p);
@@ -1899,7 +1916,7 @@ void nc_batch_options_init(nc_batch_options* o) {
     std::memset(o, 0, sizeof(*o));
     o->precision = 1;
     o->refine = 1;
-    o->krylov_dimension = 16;
+    o->krylov_dimension = 24;
     o->maximum_number_of_iterations = 100;
     o->sanity_check_threshold = 1e-12;
     o->site_convergence_threshold = 1e-12;

@@ -22,6 +22,7 @@
 
 #include "nc_common.cuh"
 #include "nc_kernels.h"
+#include "nc_ritz.cuh"
 
 namespace nc {
 
@@ -240,20 +241,7 @@ __global__ void random_kernel(long long n, uint64_t seed, cplx* __restrict__ x) 
     }
 }
 
-// ---- projected (Rayleigh-Ritz) problem ---------------------------------------
-// T = V^H H V grows by one column per Lanczos step (real symmetric: a
-// tridiagonal block plus, after a thick restart, an arrow of couplings to the
-// kept Ritz vectors).  Its eigen-decomposition T = Z Theta Z^T is kept on the
-// device between steps (the rotated matrix A ~ Theta and the accumulated
-// rotations Z, state[0..MAXT^2) and state[MAXT^2..2 MAXT^2), row-major
-// [row][col]): a new column t is taken into the current eigenbasis
-// (z = Z^T t), which leaves a diagonal matrix bordered by one row and column,
-// and one warp finishes it with cyclic Jacobi (round-robin pairing, which
-// keeps clustered Ritz values such as near-degenerate doublets orthogonal).
-// Started from an almost diagonal matrix, Jacobi needs a few sweeps instead
-// of the 6-10 of a cold start; a rotation is skipped when its off-diagonal
-// element is below the rounding level of its diagonal pair, and the sweeps
-// stop when a whole sweep skips every rotation.
+// ---- projected (Rayleigh-Ritz) problem (nc_ritz.cuh) ---------------------------
 constexpr int MAXT = 32;   // largest projected problem
 constexpr int RITZ_STATE = 2 * MAXT * MAXT;
 
@@ -264,138 +252,23 @@ struct RitzOut {
 
 // after a thick restart: A = diag(theta_0 .. theta_{k-1}), Z = I
 __global__ void restart_t_kernel(int k, const double* __restrict__ theta, double* __restrict__ state) {
-    double* A = state;
-    double* Z = state + MAXT * MAXT;
-    for (int e = threadIdx.x; e < MAXT * MAXT; e += blockDim.x) {
-        const int r = e / MAXT, c = e % MAXT;
-        A[e] = (r == c && r < k) ? theta[r] : 0.0;
-        Z[e] = (r == c) ? 1.0 : 0.0;
-    }
+    ritz_restart_state<MAXT>(k, theta, state);
 }
 
-// Adds column m-1 of T (T(i,m-1) = Re(h1_i + h2_i)) to the kept
-// decomposition of the leading (m-1) x (m-1) block and diagonalises.
-// Ritz values are ordered by `which` (SR ascending, LR descending, LM by
-// decreasing magnitude) into theta[], the matching eigenvectors of T into S
-// (m x m complex, column-major); out gets the wanted pair's value and Ritz
-// estimate beta_j |s_{m-1,0}| (beta_j = sqrt(nrm2)).
+// Adds column m-1 of T to the kept decomposition and diagonalises (one warp);
+// theta[] and S (m x m complex, column-major) receive the ordered Ritz pairs,
+// out the wanted pair's value and Ritz estimate.
 __global__ void ritz_kernel(int m, double* __restrict__ state, const cplx* __restrict__ h1,
                             const cplx* __restrict__ h2, const cplx* __restrict__ nrm2, int which,
                             RitzOut* __restrict__ out, cplx* __restrict__ S, double* __restrict__ theta) {
-    __shared__ double A[MAXT][MAXT + 1], Z[MAXT][MAXT + 1];
-    __shared__ double tcol[MAXT];
-    __shared__ double cs[MAXT / 2], sn[MAXT / 2];
-    __shared__ int pa[MAXT / 2], pb[MAXT / 2];
-    __shared__ int perm[MAXT];
-    __shared__ int rotated;
-    const int lane = threadIdx.x;
-    const int mp = m + (m & 1);
-    const double* gA = state;
-    const double* gZ = state + MAXT * MAXT;
-    // load the kept (m-1) x (m-1) decomposition, pad to mp
-    for (int r = 0; r < mp; ++r) {
-        const bool in = lane < m - 1 && r < m - 1;
-        A[r][lane] = in ? gA[r * MAXT + lane] : 0.0;
-        Z[r][lane] = in ? gZ[r * MAXT + lane] : (r == lane ? 1.0 : 0.0);
-    }
-    if (lane < m) tcol[lane] = h1[lane].x + h2[lane].x;
-    __syncwarp();
-    // border: z = Z^T t over the old rows, diagonal t_{m-1}
-    if (lane < m - 1) {
-        double z = 0.0;
-        for (int i = 0; i < m - 1; ++i) z += Z[i][lane] * tcol[i];
-        A[lane][m - 1] = z;
-        A[m - 1][lane] = z;
-    }
-    if (lane == 0) A[m - 1][m - 1] = tcol[m - 1];
-    __syncwarp();
-    int sweep = 0;
-    for (; sweep < 30; ++sweep) {
-        if (lane == 0) rotated = 0;
-        __syncwarp();
-        for (int s = 0; s < mp - 1; ++s) {
-            if (lane < mp / 2) {
-                int a, b;
-                if (lane == 0) { a = mp - 1; b = s % (mp - 1); }
-                else { a = (s + lane) % (mp - 1); b = (s - lane + mp - 1) % (mp - 1); }
-                const double apq = A[a][b], app = A[a][a], aqq = A[b][b];
-                double c = 1.0, sv = 0.0;
-                const double small = 1.1102230246251565e-16 * sqrt(fabs(app) * fabs(aqq));
-                if (fabs(apq) > small && fabs(apq) > 1e-300) {
-                    const double tau = (aqq - app) / (2.0 * apq);
-                    const double t = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-                    c = 1.0 / sqrt(1.0 + t * t);
-                    sv = t * c;
-                    rotated = 1;
-                }
-                pa[lane] = a; pb[lane] = b; cs[lane] = c; sn[lane] = sv;
-            }
-            __syncwarp();
-            if (lane < mp) {
-                for (int r = 0; r < mp / 2; ++r) {   // rows a, b of A
-                    const double sv = sn[r];
-                    if (sv == 0.0) continue;
-                    const int a = pa[r], b = pb[r];
-                    const double c = cs[r];
-                    const double xa = A[a][lane], xb = A[b][lane];
-                    A[a][lane] = c * xa - sv * xb;
-                    A[b][lane] = sv * xa + c * xb;
-                }
-            }
-            __syncwarp();
-            if (lane < mp) {
-                for (int r = 0; r < mp / 2; ++r) {   // columns a, b of A and Z
-                    const double sv = sn[r];
-                    if (sv == 0.0) continue;
-                    const int a = pa[r], b = pb[r];
-                    const double c = cs[r];
-                    const double xa = A[lane][a], xb = A[lane][b];
-                    A[lane][a] = c * xa - sv * xb;
-                    A[lane][b] = sv * xa + c * xb;
-                    const double va = Z[lane][a], vb = Z[lane][b];
-                    Z[lane][a] = c * va - sv * vb;
-                    Z[lane][b] = sv * va + c * vb;
-                }
-            }
-            __syncwarp();
-        }
-        if (!rotated) break;
-    }
-    // keep the decomposition of the m x m block for the next step
-    double* wA = state;
-    double* wZ = state + MAXT * MAXT;
-    for (int r = 0; r < m; ++r) {
-        if (lane < m) {
-            wA[r * MAXT + lane] = A[r][lane];
-            wZ[r * MAXT + lane] = Z[r][lane];
-        }
-    }
-    if (lane == 0) {
-        // order the m genuine Ritz values (a padding direction, if any, is index m)
-        for (int i = 0; i < m; ++i) perm[i] = i;
-        for (int i = 0; i < m; ++i) {
-            int best = i;
-            for (int q = i + 1; q < m; ++q) {
-                double x = A[perm[q]][perm[q]], y = A[perm[best]][perm[best]];
-                bool better = (which == WHICH_SR) ? (x < y) : (which == WHICH_LR) ? (x > y) : (fabs(x) > fabs(y));
-                if (better) best = q;
-            }
-            int t = perm[i]; perm[i] = perm[best]; perm[best] = t;
-        }
-        double tn = 0;
-        for (int i = 0; i < m; ++i) tn = fmax(tn, fabs(A[i][i]));
-        double beta = sqrt(nrm2[0].x);
-        out->theta = A[perm[0]][perm[0]];
-        out->res = beta * fabs(Z[m - 1][perm[0]]);
-        out->beta = beta;
-        out->tnorm = tn;
-        out->sweeps = sweep;
-    }
-    __syncwarp();
-    for (int r = 0; r < m; ++r) {
-        int p = perm[r];
-        if (lane < m) S[lane + m * r] = cmake(Z[lane][p], 0.0);
-        if (lane == 0) theta[r] = A[p][p];
+    __shared__ RitzSmem<MAXT> w;
+    const RitzResult r = ritz_update_warp<MAXT, true>(w, m, state, h1, h2, nrm2[0].x, which, S, m, theta);
+    if (threadIdx.x == 0) {
+        out->theta = r.theta;
+        out->res = r.res;
+        out->beta = r.beta;
+        out->tnorm = r.tnorm;
+        out->sweeps = r.sweeps;
     }
 }
 
