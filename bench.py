@@ -109,6 +109,8 @@ def parse():
     ap.add_argument("--batched-only", action="store_true", help="run only the batched-form sample")
     ap.add_argument("--batch-chains", type=int, default=256,
                     help="chains in the batched sample (the batched workload has 4096; a bounded sample)")
+    ap.add_argument("--batch-sweep-tol", type=float, default=1e-10,
+                    help="relative sweep-energy threshold of the batched sample (batch and single-chain alike)")
     ap.add_argument("--batch-plain", type=int, default=16,
                     help="chains of the batch also solved one at a time by the single-chain engine")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -415,7 +417,8 @@ def batched_sample(args):
 
     def run_batch(idx):
         with Batch([chains[k][1] for k in idx], [chains[k][2] for k in idx], seeds=[seeds[k] for k in idx],
-                   tile_table=table, maximum_sweeps=200) as b:
+                   tile_table=table, maximum_sweeps=60,
+                   sweep_convergence_threshold=args.batch_sweep_tol) as b:
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             res = b.solve()
@@ -429,6 +432,10 @@ def batched_sample(args):
     res, st, window = run_batch(list(range(len(chains))))
     log("batched: %d chains in %.1f s" % (len(chains), window))
     nplain = min(args.batch_plain, len(chains))
+    if nplain == 0:
+        return {"chains": len(chains), "chains_per_s": len(chains) / window, "window_s": window,
+                "global_steps": st["global_steps"], "lanczos_iterations": st["lanczos_iterations"],
+                "unconverged": sum(1 for r in res if not r["converged"])}
     sub = list(range(nplain))
     # plain: the single-chain FP64 engine, one chain at a time
     plain_e = []
@@ -436,7 +443,7 @@ def batched_sample(args):
     t0 = time.perf_counter()
     for k in sub:
         n, op, chi = chains[k]
-        ch = Chain(op, initial_bandwidth_dimension=chi, seed=seeds[k])
+        ch = Chain(op, initial_bandwidth_dimension=chi, seed=seeds[k], sweep_convergence_threshold=args.batch_sweep_tol)
         plain_e.append(ch.solve_levels_at_bandwidth(1)[0])
         del ch
     torch.cuda.synchronize()
@@ -450,9 +457,9 @@ def batched_sample(args):
     plain_rate = nplain / t_plain
     return {
         "workload": "XXZ chains sum J_i (XX + YY + Delta_i ZZ): J_i~U[0.5,1.5], Delta_i~U[0,2] per bond, "
-                    "N~U{8..48}, chi~U{8..128} (<= chain maximum), ground state; %d chains (bounded sample "
-                    "of the 4096-chain batch); complex64 contractions, FP64 Krylov, FP64 refinement "
-                    "sweeps" % len(chains),
+                    "N~U{8..48}, chi~U{8..128} (<= chain maximum), ground state, sweeps until the energy "
+                    "changes by < %g relative; %d chains (bounded sample of the 4096-chain batch); complex64 "
+                    "contractions, FP64 Krylov, FP64 refinement sweeps" % (args.batch_sweep_tol, len(chains)),
         "engine": "nc_batch lockstep: one grouped launch per contraction stage, Lanczos iteration as "
                   "one CUDA graph replay",
         "chains": len(chains), "unconverged": sum(1 for r in res if not r["converged"]),

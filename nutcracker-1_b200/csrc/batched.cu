@@ -397,8 +397,11 @@ __device__ __forceinline__ void block_sum_c(double (&ar)[NK], double (&ai)[NK], 
 }
 
 // PASS 0: part = V^H w;  PASS 1: w -= V h1, part = V^H w;  PASS 2: w -= V h2, part[0] = |w|^2.
-// The update runs per element over all k; the dot products per warp over
-// its k (k = warp, warp + 8, ...), each a fixed-order sum over the chunk.
+// Each thread keeps its (at most kVecChunk / kLzT) elements of w in
+// registers; the dot products run four basis vectors at a time, so that every
+// thread has many independent loads in flight, each a fixed-order sum over
+// the chunk.
+constexpr int kEpt = kVecChunk / kLzT;
 template <int PASS>
 __global__ void __launch_bounds__(kLzT) lz_cgs_kernel(const VChunk* __restrict__ chunks, const int* __restrict__ nchunks,
                                                       const LzChain* __restrict__ ch, LzState* __restrict__ st,
@@ -406,7 +409,6 @@ __global__ void __launch_bounds__(kLzT) lz_cgs_kernel(const VChunk* __restrict__
     __shared__ cplx red[kLzW * (kMaxKrylov + 1)];
     __shared__ cplx hs[kMaxKrylov + 1];
     const int total = *nchunks;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
         const VChunk c = chunks[t];
         const LzState& S = st[c.chain];
@@ -416,38 +418,57 @@ __global__ void __launch_bounds__(kLzT) lz_cgs_kernel(const VChunk* __restrict__
         __syncthreads();
         if (PASS > 0 && threadIdx.x < nk) hs[threadIdx.x] = (PASS == 1) ? S.h1[threadIdx.x] : S.h2[threadIdx.x];
         __syncthreads();
-        double nr[1] = {0}, ni[1] = {0};
+        const int end = c.off + c.len;
+        cplx wv[kEpt];
+#pragma unroll
+        for (int e = 0; e < kEpt; ++e) {
+            const int i = c.off + threadIdx.x + e * kLzT;
+            wv[e] = (i < end) ? C.w[i] : cmake(0, 0);
+        }
         if (PASS > 0) {
-            for (int i = c.off + threadIdx.x; i < c.off + c.len; i += kLzT) {
-                double wr = C.w[i].x, wi = C.w[i].y;
-                for (int k = 0; k < nk; ++k) {
-                    const cplx v = C.V[(long long)k * C.n + i], h = hs[k];
-                    wr -= v.x * h.x - v.y * h.y;
-                    wi -= v.x * h.y + v.y * h.x;
+            double nr[1] = {0}, ni[1] = {0};
+            for (int k = 0; k < nk; ++k) {
+                const cplx h = hs[k];
+                const cplx* Vk = C.V + (long long)k * C.n;
+#pragma unroll
+                for (int e = 0; e < kEpt; ++e) {
+                    const int i = c.off + threadIdx.x + e * kLzT;
+                    if (i < end) {
+                        const cplx v = Vk[i];
+                        wv[e].x -= v.x * h.x - v.y * h.y;
+                        wv[e].y -= v.x * h.y + v.y * h.x;
+                    }
                 }
-                C.w[i] = cmake(wr, wi);
-                nr[0] = fma(wr, wr, fma(wi, wi, nr[0]));
-            }
-        }
-        if (PASS == 2) {
-            block_sum_c<1>(nr, ni, 1, red, part + (long long)t * kPartStride);
-            continue;
-        }
-        __syncthreads();   // the updated w of the whole chunk is visible
-        for (int k = warp; k < nk; k += kLzW) {
-            const cplx* Vk = C.V + (long long)k * C.n;
-            double ar = 0, ai = 0;
-            for (int i = c.off + lane; i < c.off + c.len; i += 32) {
-                const cplx v = Vk[i], w = C.w[i];   // conj(v) * w
-                ar = fma(v.x, w.x, fma(v.y, w.y, ar));
-                ai = fma(v.x, w.y, fma(-v.y, w.x, ai));
             }
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                ar += __shfl_xor_sync(0xffffffffu, ar, o);
-                ai += __shfl_xor_sync(0xffffffffu, ai, o);
+            for (int e = 0; e < kEpt; ++e) {
+                const int i = c.off + threadIdx.x + e * kLzT;
+                if (i < end) {
+                    C.w[i] = wv[e];
+                    nr[0] = fma(wv[e].x, wv[e].x, fma(wv[e].y, wv[e].y, nr[0]));
+                }
             }
-            if (lane == 0) part[(long long)t * kPartStride + k] = cmake(ar, ai);
+            if (PASS == 2) block_sum_c<1>(nr, ni, 1, red, part + (long long)t * kPartStride);
+        }
+        if constexpr (PASS < 2) for (int k0 = 0; k0 < nk; k0 += 4) {
+            const int kc = min(4, nk - k0);
+            double ar[4] = {0, 0, 0, 0}, ai[4] = {0, 0, 0, 0};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if (q < kc) {
+                    const cplx* Vk = C.V + (long long)(k0 + q) * C.n;
+#pragma unroll
+                    for (int e = 0; e < kEpt; ++e) {
+                        const int i = c.off + threadIdx.x + e * kLzT;
+                        if (i < end) {
+                            const cplx v = Vk[i];   // conj(v) * w
+                            ar[q] = fma(v.x, wv[e].x, fma(v.y, wv[e].y, ar[q]));
+                            ai[q] = fma(v.x, wv[e].y, fma(-v.y, wv[e].x, ai[q]));
+                        }
+                    }
+                }
+            }
+            block_sum_c<4>(ar, ai, kc, red, part + (long long)t * kPartStride + k0);
         }
     }
 }

@@ -36,7 +36,10 @@ pytestmark = pytest.mark.gpu
 
 def _fixture(name):
     with open(os.path.join(HERE, "golden", "scale_levels.json")) as f:
-        return json.load(f)[name]
+        data = json.load(f)
+    if name not in data:
+        pytest.skip("oracle fixture %s not generated (tests/golden/make_scale_fixtures.py %s)" % (name, name))
+    return data[name]
 
 
 def _solve_levels(name, precision=0):
