@@ -567,8 +567,9 @@ typedef struct {
     uint64_t device_bytes;            /* the batch's device allocation */
     double seconds;                   /* wall time of the last nc_batch_solve */
     double seconds_moves, seconds_solves;   /* with time_phases: gauge moves + environments, site solves */
-    uint64_t restart_rounds;          /* Lanczos restarts of the lockstep solver (every chain at once) */
-    uint64_t max_iterations_per_step; /* most Lanczos iterations one global step needed */
+    uint64_t continued_solves;        /* site solves carried into a following step (a step gives every
+                                         solving chain at most 8 Lanczos iterations) */
+    uint64_t max_iterations_per_step; /* most Lanczos iterations one global step ran */
 } nc_batch_stats;
 typedef struct nc_batch nc_batch;
 

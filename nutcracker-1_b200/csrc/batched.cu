@@ -78,6 +78,7 @@ struct LzState {
     int stall;      // 1: basis full, waiting for a restart
     int adv;        // 1: the next basis vector is to be written
     int restarts, matvecs, fail, accept;
+    int fin;        // 1: the solve's result has been taken (or there is no solve)
     double theta, res, beta, tnorm, xnorm, energy;
     cplx h1[kMaxKrylov + 1], h2[kMaxKrylov + 1];
     double wn2;
@@ -561,19 +562,37 @@ __global__ void lz_inc_kernel(int nchains, LzState* __restrict__ st, int* __rest
 
 // ---- solve set-up, restarts and the result ------------------------------------
 
-// Per chain: start a solve (active[c] != 0) or sit this step out.
+// Per chain: solving[c] = 1 starts a solve, 2 continues the one in progress,
+// 0 sits this step out.
 __global__ void lz_init_kernel(int nchains, const int* __restrict__ solving, LzState* __restrict__ st) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nchains) return;
     LzState& S = st[c];
+    if (solving[c] == 2) return;
+    const bool start = solving[c] == 1;
     S.j = 0;
-    S.done = solving[c] ? 0 : 1;
+    S.done = start ? 0 : 1;
     S.stall = 0;
     S.adv = 0;
     S.restarts = 0;
     S.matvecs = 0;
     S.fail = 0;
     S.accept = 0;
+    S.fin = start ? 0 : 1;
+}
+
+// After a step's iterations: the chains whose solve ended (converged or
+// failed) and whose result was taken this step are reported to the host,
+// with their energies.
+__global__ void lz_finish_kernel(int nchains, const int* __restrict__ solving, LzState* __restrict__ st,
+                                 int* __restrict__ finished, double* __restrict__ energy) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nchains) return;
+    LzState& S = st[c];
+    const int f = (solving[c] && S.done && !S.fin) ? 1 : 0;
+    if (f) S.fin = 1;
+    finished[c] = f;
+    energy[c] = S.energy;
 }
 
 // MODE 0: V_0 = x (the guess), part = |x|^2   (chains with !done)
@@ -589,7 +608,8 @@ __global__ void __launch_bounds__(kLzT) lz_form_kernel(const VChunk* __restrict_
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
         const VChunk c = chunks[t];
         const LzState& S = st[c.chain];
-        const bool on = (MODE == 0) ? !S.done : (solving[c.chain] && S.done && !S.fail);
+        const bool on = (MODE == 0) ? (solving[c.chain] == 1 && !S.done)
+                                    : (solving[c.chain] && S.done && !S.fin && !S.fail);
         if (!on) continue;
         const LzChain C = ch[c.chain];
         const int nk = S.j + 1;
@@ -627,7 +647,7 @@ __global__ void lz_norm_kernel(int nchains, const LzChain* __restrict__ ch, LzSt
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nchains) return;
     LzState& S = st[c];
-    const bool on = (MODE == 0) ? !S.done : (solving[c] && S.done && !S.fail);
+    const bool on = (MODE == 0) ? (solving[c] == 1 && !S.done) : (solving[c] && S.done && !S.fin && !S.fail);
     if (!on) return;
     const LzChain C = ch[c];
     double x = 0;
@@ -659,11 +679,11 @@ __global__ void __launch_bounds__(kLzT) lz_scale_kernel(const VChunk* __restrict
         const LzState& S = st[c.chain];
         const LzChain C = ch[c.chain];
         if (MODE == 0) {
-            if (S.done) continue;
+            if (solving[c.chain] != 1 || S.done) continue;
             const double f = 1.0 / S.xnorm;
             for (int i = c.off + threadIdx.x; i < c.off + c.len; i += kLzT) C.V[i] = cscale(C.V[i], f);
         } else {
-            if (!(solving[c.chain] && S.accept)) continue;
+            if (!(solving[c.chain] && S.done && !S.fin && !S.fail && S.accept)) continue;
             const double f = 1.0 / S.xnorm;
             for (int i = c.off + threadIdx.x; i < c.off + c.len; i += kLzT) C.x[i] = cscale(C.w[i], f);
         }
@@ -941,19 +961,6 @@ __global__ void random_fill_kernel(cplx* x, long long n, uint64_t seed) {
         x[e] = cmake(unit_rand(seed, 2 * e), unit_rand(seed, 2 * e + 1));
 }
 
-// Chains still iterating (neither converged, failed nor waiting for a
-// restart); one block.
-__global__ void count_kernel(int nchains, const LzState* __restrict__ st, int* __restrict__ active) {
-    __shared__ int cnt;
-    if (threadIdx.x == 0) cnt = 0;
-    __syncthreads();
-    int local = 0;
-    for (int c = threadIdx.x; c < nchains; c += blockDim.x) local += (!st[c].done && !st[c].stall) ? 1 : 0;
-    atomicAdd(&cnt, local);
-    __syncthreads();
-    if (threadIdx.x == 0) *active = cnt;
-}
-
 __global__ void set_one_kernel(cplx* const* ptrs, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) *ptrs[i] = cmake(1, 0);
@@ -1175,7 +1182,7 @@ struct ChainHost {
     size_t max_site = 0;
     // sweep state
     int cur = 0, dir = 1;
-    bool optimized = false, converged = false;
+    bool optimized = false, converged = false, solving = false;
     int sweeps = 0, phase_sweeps = 0, mixed_sweeps = 0, fp64_sweeps = 0;
     double prev = NAN, energy = NAN;
     bool unconverged = false;
@@ -1205,7 +1212,8 @@ struct Engine {
     DevArray<LzChain> d_lz;
     DevArray<LzState> d_st;
     DevArray<LzRitz> d_rz;
-    DevArray<int> d_solving, d_active;
+    DevArray<int> d_solving, d_active, d_finished;
+    DevArray<double> d_energy;
     DevArray<cplx> d_part, d_part_n;
     DevArray<NormJob> d_norm_jobs;
     DevArray<QrProb> d_qr;
@@ -1216,6 +1224,7 @@ struct Engine {
     std::vector<NormJob> h_norm_jobs;
     std::vector<QrProb> h_qr;
     int* h_active = nullptr;   // pinned
+    int* h_finished = nullptr;   // pinned, one per chain
     double* h_energy = nullptr;   // pinned, one per chain
     LzState* h_state = nullptr;   // pinned, used for stats reads
 
@@ -1225,7 +1234,7 @@ struct Engine {
 
     // statistics
     uint64_t global_steps = 0, lanczos_iterations = 0, graph_launches = 0, launches = 0;
-    uint64_t restart_rounds = 0, max_iterations_per_step = 0;
+    uint64_t continued_solves = 0, max_iterations_per_step = 0;
     double seconds = 0, seconds_moves = 0, seconds_solves = 0;   // the last two with time_phases
 
     ~Engine() {
@@ -1233,6 +1242,7 @@ struct Engine {
         if (graph) cudaGraphDestroy(graph);
         if (pool) cudaFree(pool);
         if (h_active) cudaFreeHost(h_active);
+        if (h_finished) cudaFreeHost(h_finished);
         if (h_energy) cudaFreeHost(h_energy);
         if (h_state) cudaFreeHost(h_state);
         if (stream) cudaStreamDestroy(stream);
@@ -1389,6 +1399,8 @@ struct Engine {
         d_st.reserve(B);
         d_rz.reserve(B);
         d_solving.reserve(B);
+        d_finished.reserve(B);
+        d_energy.reserve(B);
         d_active.reserve(1);
         d_part.reserve(nchunk_cap * kPartStride);
         d_part_n.reserve(nchunk_cap * kPartStride);
@@ -1400,6 +1412,7 @@ struct Engine {
         h_solving.assign(B, 0);
         h_norm_jobs.assign(B, NormJob{nullptr, 0, 0});
         NC_CUDA(cudaMallocHost(&h_active, sizeof(int)));
+        NC_CUDA(cudaMallocHost(&h_finished, B * sizeof(int)));
         NC_CUDA(cudaMallocHost(&h_energy, B * sizeof(double)));
         NC_CUDA(cudaMallocHost(&h_state, B * sizeof(LzState)));
         NC_CUDA(cudaMemsetAsync(d_st.p, 0, B * sizeof(LzState), stream));
@@ -1673,13 +1686,17 @@ struct Engine {
         lz_reduce_kernel<2><<<cb, 256, 0, stream>>>(B, d_lz.p, st, d_part.p);
         lz_ritz_kernel<<<B, 32, 0, stream>>>(B, d_lz.p, st, d_rz.p, d_active.p);
         lz_next_kernel<<<grid_vec, kLzT, 0, stream>>>(lz_chunks.d.p, lz_chunks.d_count.p, d_lz.p, st);
+        // thick restart of the chains whose basis filled in this iteration
+        lz_restart_form_kernel<<<grid_vec, kLzT, 0, stream>>>(lz_chunks.d.p, lz_chunks.d_count.p, d_lz.p, st, d_rz.p);
+        lz_restart_copy_kernel<<<grid_vec, kLzT, 0, stream>>>(lz_chunks.d.p, lz_chunks.d_count.p, d_lz.p, st);
+        lz_restart_state_kernel<<<B, 32, 0, stream>>>(B, d_lz.p, st, d_rz.p);
         lz_inc_kernel<<<tb, 256, 0, stream>>>(B, st, d_active.p);
         cudaError_t e = cudaStreamEndCapture(stream, &graph);
         NC_CUDA(e);
         NC_CHECK_LAUNCH();
         NC_CUDA(cudaGraphInstantiate(&graph_exec, graph, 0));
     }
-    static constexpr int kGraphKernels = 12;
+    static constexpr int kGraphKernels = 15;
 
     int read_active() {
         NC_CUDA(cudaMemcpyAsync(h_active, d_active.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
@@ -1687,14 +1704,23 @@ struct Engine {
         return *h_active;
     }
 
-    void do_solves(const std::vector<int>& solvers, int prec, double site_tol, double sanity) {
-        if (solvers.empty()) return;
+    // One step of the site solves: `starting` chains begin a solve at their
+    // centre (the guess is the site), `continuing` ones carry on with the
+    // basis they have.  Every solving chain gets at most `iteration_cap`
+    // Lanczos iterations in this step (thick restarts happen inside the
+    // graph); a chain whose solve ends (converged or failed) has its result
+    // taken and is returned in `finished` with its energy, the others continue
+    // in the next step, so one slow solve does not hold the other chains.
+    void do_solves(const std::vector<int>& starting, const std::vector<int>& continuing, int prec,
+                   double site_tol, double sanity, std::vector<int>& finished) {
+        finished.clear();
+        if (starting.empty() && continuing.empty()) return;
         const int B = (int)chains.size();
         const int tb = (B + 255) / 256;
         g_a.clear(); g_c.clear(); m_h.clear(); lz_chunks.clear();
         std::fill(h_solving.begin(), h_solving.end(), 0);
         for (int c = 0; c < B; ++c) h_lz[c].ccount = 0;
-        for (int c : solvers) {
+        auto add = [&](int c, int flag) {
             ChainHost& ch = chains[c];
             const int i = ch.cur;
             const MpoDev& op = ch.ops[i];
@@ -1723,8 +1749,10 @@ struct Engine {
             z.keep = std::max(1, std::min(std::max(4, z.m_max / 3), z.m_max - 2));
             z.Y = ch.Y;
             z.maxit = (int)std::max<uint32_t>(1, opt.maximum_number_of_iterations);
-            h_solving[c] = 1;
-        }
+            h_solving[c] = flag;
+        };
+        for (int c : starting) add(c, 1);
+        for (int c : continuing) add(c, 2);
         g_a.upload(stream);
         g_c.upload(stream);
         m_h.upload(stream);
@@ -1740,44 +1768,35 @@ struct Engine {
         lz_scale_kernel<0><<<grid_vec, kLzT, 0, stream>>>(lz_chunks.d.p, lz_chunks.d_count.p, d_lz.p, st, d_solving.p);
         NC_CHECK_LAUNCH();
         launches += 4;
-        const int m_max = (int)opt.krylov_dimension;
         const int check_every = 4;
         uint64_t iters = 0;
-        for (;;) {
-            int active = 1;
-            for (int it = 0; it < m_max; ++it) {
-                NC_CUDA(cudaGraphLaunch(graph_exec, stream));
-                graph_launches++;
-                lanczos_iterations++;
-                iters++;
-                launches += kGraphKernels;
-                if ((it + 1) % check_every == 0 || it + 1 == m_max) {
-                    active = read_active();
-                    if (active == 0) break;
-                }
-            }
-            // chains whose basis is full restart from their Ritz vector
-            // thick restart of the chains whose basis is full (the others are skipped)
-            lz_restart_form_kernel<<<grid_vec, kLzT, 0, stream>>>(lz_chunks.d.p, lz_chunks.d_count.p, d_lz.p, st, d_rz.p);
-            lz_restart_copy_kernel<<<grid_vec, kLzT, 0, stream>>>(lz_chunks.d.p, lz_chunks.d_count.p, d_lz.p, st);
-            lz_restart_state_kernel<<<B, 32, 0, stream>>>(B, d_lz.p, st, d_rz.p);
-            NC_CHECK_LAUNCH();
-            launches += 3;
-            // anything left to iterate?
-            count_kernel<<<1, 256, 0, stream>>>(B, st, d_active.p);
-            NC_CHECK_LAUNCH();
-            launches++;
-            if (read_active() == 0) break;
-            restart_rounds++;
+        for (int it = 0; it < iteration_cap; ++it) {
+            NC_CUDA(cudaGraphLaunch(graph_exec, stream));
+            graph_launches++;
+            lanczos_iterations++;
+            iters++;
+            launches += kGraphKernels;
+            if ((it + 1) % check_every == 0 && read_active() == 0) break;
         }
         max_iterations_per_step = std::max(max_iterations_per_step, iters);
+        // the results of the solves that ended
         lz_form_kernel<2><<<grid_vec, kLzT, 0, stream>>>(lz_chunks.d.p, lz_chunks.d_count.p, d_lz.p, st, d_rz.p, d_solving.p,
                                                          d_part.p);
         lz_norm_kernel<2><<<tb, 256, 0, stream>>>(B, d_lz.p, st, d_solving.p, d_part.p, sanity);
         lz_scale_kernel<2><<<grid_vec, kLzT, 0, stream>>>(lz_chunks.d.p, lz_chunks.d_count.p, d_lz.p, st, d_solving.p);
+        lz_finish_kernel<<<tb, 256, 0, stream>>>(B, d_solving.p, st, d_finished.p, d_energy.p);
         NC_CHECK_LAUNCH();
-        launches += 3;
+        launches += 4;
+        NC_CUDA(cudaMemcpyAsync(h_finished, d_finished.p, B * sizeof(int), cudaMemcpyDeviceToHost, stream));
+        NC_CUDA(cudaMemcpyAsync(h_energy, d_energy.p, B * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        NC_CUDA(cudaStreamSynchronize(stream));
+        for (int c = 0; c < B; ++c)
+            if (h_solving[c] && h_finished[c]) {
+                finished.push_back(c);
+                chains[c].energy = h_energy[c];
+            }
     }
+    int iteration_cap = 8;
 
     // ---- sweeps ---------------------------------------------------------------
     // Every chain sweeps (chain.cpp:147-163) until its sweep energy settles
@@ -1790,49 +1809,50 @@ struct Engine {
             ch.dir = 1;
             ch.optimized = false;
             ch.converged = false;
+            ch.solving = false;
             ch.phase_sweeps = 0;
             ch.prev = NAN;
         }
-        std::vector<int> movers, solvers;
+        std::vector<int> movers, starting, continuing, finished;
         for (;;) {
             movers.clear();
-            solvers.clear();
+            starting.clear();
+            continuing.clear();
             for (int c = 0; c < B; ++c) {
                 ChainHost& ch = chains[c];
                 if (ch.converged) continue;
+                if (ch.solving) {
+                    continuing.push_back(c);
+                    continue;
+                }
                 if (ch.optimized) {
                     if (ch.dir > 0 && ch.cur + 1 >= ch.N) ch.dir = -1;
                     movers.push_back(c);
                 }
-                solvers.push_back(c);
+                starting.push_back(c);
             }
-            if (solvers.empty()) break;
+            if (starting.empty() && continuing.empty()) break;
             global_steps++;
+            continued_solves += continuing.size();
             if (opt.time_phases) {
                 auto t0 = std::chrono::steady_clock::now();
                 do_moves(movers, prec);
                 NC_CUDA(cudaStreamSynchronize(stream));
                 auto t1 = std::chrono::steady_clock::now();
-                do_solves(solvers, prec, site_tol, sanity);
-                NC_CUDA(cudaStreamSynchronize(stream));
+                do_solves(starting, continuing, prec, site_tol, sanity, finished);
                 auto t2 = std::chrono::steady_clock::now();
                 seconds_moves += std::chrono::duration<double>(t1 - t0).count();
                 seconds_solves += std::chrono::duration<double>(t2 - t1).count();
             } else {
                 do_moves(movers, prec);
-                do_solves(solvers, prec, site_tol, sanity);
+                do_solves(starting, continuing, prec, site_tol, sanity, finished);
             }
-            bool sweep_end = false;
-            for (int c : solvers) {
+            for (int c : starting) chains[c].solving = true;
+            for (int c : finished) {
                 ChainHost& ch = chains[c];
+                ch.solving = false;
                 ch.optimized = true;
                 ch.site_solves++;
-                if (ch.dir < 0 && ch.cur == 0) sweep_end = true;
-            }
-            if (!sweep_end) continue;
-            read_states();
-            for (int c : solvers) {
-                ChainHost& ch = chains[c];
                 if (!(ch.dir < 0 && ch.cur == 0)) continue;
                 // a sweep has ended at site 0
                 ch.dir = 1;
@@ -1840,7 +1860,7 @@ struct Engine {
                 ch.phase_sweeps++;
                 if (prec) ch.mixed_sweeps++;
                 else ch.fp64_sweeps++;
-                const double now = h_energy[c];
+                const double now = ch.energy;
                 if (!std::isnan(ch.prev) && !outside_tolerance(ch.prev, now, sweep_tol)) {
                     ch.converged = true;
                 } else if (max_sweeps && (uint32_t)ch.phase_sweeps >= max_sweeps) {
@@ -2017,7 +2037,7 @@ int nc_batch_get_stats(nc_batch* b, nc_batch_stats* st) {
     st->seconds = b->e.seconds;
     st->seconds_moves = b->e.seconds_moves;
     st->seconds_solves = b->e.seconds_solves;
-    st->restart_rounds = b->e.restart_rounds;
+    st->continued_solves = b->e.continued_solves;
     st->max_iterations_per_step = b->e.max_iterations_per_step;
     st->device_bytes = b->e.pool_bytes;
     NC_ABI_END

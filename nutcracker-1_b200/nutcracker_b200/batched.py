@@ -55,7 +55,7 @@ class nc_batch_stats(ct.Structure):
         ("graph_launches", ct.c_uint64), ("kernel_launches", ct.c_uint64),
         ("device_bytes", ct.c_uint64), ("seconds", ct.c_double),
         ("seconds_moves", ct.c_double), ("seconds_solves", ct.c_double),
-        ("restart_rounds", ct.c_uint64), ("max_iterations_per_step", ct.c_uint64),
+        ("continued_solves", ct.c_uint64), ("max_iterations_per_step", ct.c_uint64),
     ]
 
 
