@@ -1068,6 +1068,35 @@ struct DevArray {
     ~DevArray() { if (p) cudaFree(p); }
 };
 
+// Pinned staging of the per-step uploads: host data is copied into pinned
+// memory and the copy is enqueued asynchronously (a copy from pageable memory
+// waits for the stream, which would serialise the host with the device at
+// every upload).  The area is reused from its start after each
+// synchronisation of the stream; when it runs out it synchronises itself.
+struct Stager {
+    char* base = nullptr;
+    size_t cap = 0, used = 0;
+    ~Stager() { if (base) cudaFreeHost(base); }
+    void reset() { used = 0; }
+    void copy(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+        if (!bytes) return;
+        size_t off = (used + 255) & ~(size_t)255;
+        if (off + bytes > cap) {
+            NC_CUDA(cudaStreamSynchronize(s));
+            off = 0;
+            if (bytes > cap) {
+                if (base) NC_CUDA(cudaFreeHost(base));
+                base = nullptr;
+                cap = std::max(bytes, (size_t)16 << 20);
+                NC_CUDA(cudaMallocHost(&base, cap));
+            }
+        }
+        std::memcpy(base + off, src, bytes);
+        used = off + bytes;
+        NC_CUDA(cudaMemcpyAsync(dst, base + off, bytes, cudaMemcpyHostToDevice, s));
+    }
+};
+
 // A grouped-GEMM work list: problems, tile prefix sums, tile -> problem map.
 struct GemmList {
     std::vector<GProb> h;
@@ -1084,7 +1113,7 @@ struct GemmList {
     }
     int tiles_of(const GProb& g) const { return ((g.M + kTileM[g.cfg] - 1) / kTileM[g.cfg]) * g.tiles_n; }
     // Uploads the list (the device buffers keep their addresses once reserved).
-    void upload(cudaStream_t s) {
+    void upload(Stager& sg, cudaStream_t s) {
         h_prefix.assign(h.size() + 1, 0);
         for (size_t i = 0; i < h.size(); ++i) h_prefix[i + 1] = h_prefix[i] + tiles_of(h[i]);
         const int total = h_prefix.back();
@@ -1093,12 +1122,12 @@ struct GemmList {
             for (int t = h_prefix[i]; t < h_prefix[i + 1]; ++t) h_tile[t] = (int)i;
         NC_ARG(h.size() <= d_probs.cap && (size_t)total <= d_tile.cap, "batched work list exceeds its capacity");
         if (!h.empty()) {
-            NC_CUDA(cudaMemcpyAsync(d_probs.p, h.data(), h.size() * sizeof(GProb), cudaMemcpyHostToDevice, s));
-            NC_CUDA(cudaMemcpyAsync(d_prefix.p, h_prefix.data(), h_prefix.size() * sizeof(int), cudaMemcpyHostToDevice, s));
-            NC_CUDA(cudaMemcpyAsync(d_tile.p, h_tile.data(), (size_t)total * sizeof(int), cudaMemcpyHostToDevice, s));
+            sg.copy(d_probs.p, h.data(), h.size() * sizeof(GProb), s);
+            sg.copy(d_prefix.p, h_prefix.data(), h_prefix.size() * sizeof(int), s);
+            sg.copy(d_tile.p, h_tile.data(), (size_t)total * sizeof(int), s);
         }
         h_total = total;
-        NC_CUDA(cudaMemcpyAsync(d_count.p, &h_total, sizeof(int), cudaMemcpyHostToDevice, s));
+        sg.copy(d_count.p, &h_total, sizeof(int), s);
     }
     int h_total = 0;
     void reserve(size_t probs, size_t tiles) {
@@ -1118,7 +1147,7 @@ struct MixList {
     int h_total = 0;
     void clear() { h.clear(); }
     void add(const MixProb& m) { h.push_back(m); }
-    void upload(cudaStream_t s) {
+    void upload(Stager& sg, cudaStream_t s) {
         h_items.clear();
         for (size_t i = 0; i < h.size(); ++i) {
             const long long chunks = (h[i].total + kMixChunk - 1) / kMixChunk;
@@ -1126,11 +1155,11 @@ struct MixList {
         }
         NC_ARG(h.size() <= d_probs.cap && h_items.size() <= d_items.cap, "batched mix list exceeds its capacity");
         if (!h.empty()) {
-            NC_CUDA(cudaMemcpyAsync(d_probs.p, h.data(), h.size() * sizeof(MixProb), cudaMemcpyHostToDevice, s));
-            NC_CUDA(cudaMemcpyAsync(d_items.p, h_items.data(), h_items.size() * sizeof(int2), cudaMemcpyHostToDevice, s));
+            sg.copy(d_probs.p, h.data(), h.size() * sizeof(MixProb), s);
+            sg.copy(d_items.p, h_items.data(), h_items.size() * sizeof(int2), s);
         }
         h_total = (int)h_items.size();
-        NC_CUDA(cudaMemcpyAsync(d_count.p, &h_total, sizeof(int), cudaMemcpyHostToDevice, s));
+        sg.copy(d_count.p, &h_total, sizeof(int), s);
     }
     void reserve(size_t probs, size_t items) {
         d_probs.reserve(probs);
@@ -1152,11 +1181,11 @@ struct ChunkList {
             h.push_back(VChunk{chain, (int)off, (int)std::min<long long>(kVecChunk, n - off)});
         return {start, (int)h.size() - start};
     }
-    void upload(cudaStream_t s) {
+    void upload(Stager& sg, cudaStream_t s) {
         NC_ARG(h.size() <= d.cap, "batched chunk list exceeds its capacity");
-        if (!h.empty()) NC_CUDA(cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(VChunk), cudaMemcpyHostToDevice, s));
+        if (!h.empty()) sg.copy(d.p, h.data(), h.size() * sizeof(VChunk), s);
         h_total = (int)h.size();
-        NC_CUDA(cudaMemcpyAsync(d_count.p, &h_total, sizeof(int), cudaMemcpyHostToDevice, s));
+        sg.copy(d_count.p, &h_total, sizeof(int), s);
     }
     void reserve(size_t n) {
         d.reserve(n);
@@ -1228,6 +1257,7 @@ struct Engine {
     double* h_energy = nullptr;   // pinned, one per chain
     LzState* h_state = nullptr;   // pinned, used for stats reads
 
+    Stager stager;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     int grid_gemm = 0, grid_mix = 0, grid_vec = 0, grid_qr = 0;
@@ -1498,9 +1528,8 @@ struct Engine {
 
     // Normalise one vector per listed chain (nrm_chunks / h_norm_jobs filled).
     void run_normalise() {
-        nrm_chunks.upload(stream);
-        NC_CUDA(cudaMemcpyAsync(d_norm_jobs.p, h_norm_jobs.data(), h_norm_jobs.size() * sizeof(NormJob),
-                                cudaMemcpyHostToDevice, stream));
+        nrm_chunks.upload(stager, stream);
+        stager.copy(d_norm_jobs.p, h_norm_jobs.data(), h_norm_jobs.size() * sizeof(NormJob), stream);
         norm_partial_kernel<<<grid_vec, kLzT, 0, stream>>>(nrm_chunks.d.p, nrm_chunks.d_count.p, d_norm_jobs.p,
                                                            d_part_n.p);
         NC_CHECK_LAUNCH();
@@ -1513,8 +1542,8 @@ struct Engine {
     void run_qr() {
         const int n = (int)h_qr.size();
         if (n == 0) return;
-        NC_CUDA(cudaMemcpyAsync(d_qr.p, h_qr.data(), h_qr.size() * sizeof(QrProb), cudaMemcpyHostToDevice, stream));
-        NC_CUDA(cudaMemcpyAsync(d_qr_count.p, &qr_count_host, sizeof(int), cudaMemcpyHostToDevice, stream));
+        stager.copy(d_qr.p, h_qr.data(), h_qr.size() * sizeof(QrProb), stream);
+        stager.copy(d_qr_count.p, &qr_count_host, sizeof(int), stream);
         batched_qr_kernel<<<std::min(grid_qr, n), kQrThreads, 0, stream>>>(d_qr.p, d_qr_count.p);
         NC_CHECK_LAUNCH();
         launches++;
@@ -1541,7 +1570,7 @@ struct Engine {
             ones.push_back(ch.L[0]);
             ones.push_back(ch.R[ch.N - 1]);
         }
-        NC_CUDA(cudaMemcpyAsync(d_ones.p, ones.data(), ones.size() * sizeof(cplx*), cudaMemcpyHostToDevice, stream));
+        stager.copy(d_ones.p, ones.data(), ones.size() * sizeof(cplx*), stream);
         set_one_kernel<<<((int)ones.size() + 255) / 256, 256, 0, stream>>>(d_ones.p, (int)ones.size());
         NC_CHECK_LAUNCH();
         // the centre
@@ -1606,9 +1635,9 @@ struct Engine {
     }
 
     void upload_moves() {
-        g_mv1.upload(stream);
-        g_mv2.upload(stream);
-        m_mv.upload(stream);
+        g_mv1.upload(stager, stream);
+        g_mv2.upload(stager, stream);
+        m_mv.upload(stager, stream);
     }
 
     uint64_t seed_of(const ChainHost& ch, int site) const {
@@ -1753,12 +1782,12 @@ struct Engine {
         };
         for (int c : starting) add(c, 1);
         for (int c : continuing) add(c, 2);
-        g_a.upload(stream);
-        g_c.upload(stream);
-        m_h.upload(stream);
-        lz_chunks.upload(stream);
-        NC_CUDA(cudaMemcpyAsync(d_lz.p, h_lz.data(), B * sizeof(LzChain), cudaMemcpyHostToDevice, stream));
-        NC_CUDA(cudaMemcpyAsync(d_solving.p, h_solving.data(), B * sizeof(int), cudaMemcpyHostToDevice, stream));
+        g_a.upload(stager, stream);
+        g_c.upload(stager, stream);
+        m_h.upload(stager, stream);
+        lz_chunks.upload(stager, stream);
+        stager.copy(d_lz.p, h_lz.data(), B * sizeof(LzChain), stream);
+        stager.copy(d_solving.p, h_solving.data(), B * sizeof(int), stream);
         capture_graph();
         LzState* st = d_st.p;
         lz_init_kernel<<<tb, 256, 0, stream>>>(B, d_solving.p, st);
@@ -1790,6 +1819,7 @@ struct Engine {
         NC_CUDA(cudaMemcpyAsync(h_finished, d_finished.p, B * sizeof(int), cudaMemcpyDeviceToHost, stream));
         NC_CUDA(cudaMemcpyAsync(h_energy, d_energy.p, B * sizeof(double), cudaMemcpyDeviceToHost, stream));
         NC_CUDA(cudaStreamSynchronize(stream));
+        stager.reset();   // every staged upload has been consumed
         for (int c = 0; c < B; ++c)
             if (h_solving[c] && h_finished[c]) {
                 finished.push_back(c);
@@ -2085,6 +2115,7 @@ int nc_batch_autotune_stage(uint32_t stage, uint32_t chi, uint32_t D, uint32_t d
     NC_CUDA(cudaEventCreate(&g.a));
     NC_CUDA(cudaEventCreate(&g.b));
     GemmList list;
+    Stager sg;
     list.reserve((size_t)problems * count, (size_t)problems * count * ((M + 15) / 16) * ((N + 15) / 16));
     for (int cfg = 0; cfg < kTileConfigs; ++cfg) {
         list.clear();
@@ -2097,7 +2128,7 @@ int nc_batch_autotune_stage(uint32_t stage, uint32_t chi, uint32_t D, uint32_t d
                 x.C = C + ec * ((size_t)p * count + q); x.ldc = M;
                 list.add(x);
             }
-        list.upload(s);
+        list.upload(sg, s);
         for (int w = 0; w < 2; ++w)
             grouped_gemm_kernel<<<grid, kGemmThreads, kGemmSmem, s>>>(list.d_probs.p, list.d_prefix.p, list.d_tile.p,
                                                                        list.d_count.p, nullptr);
