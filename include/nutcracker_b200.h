@@ -570,6 +570,7 @@ typedef struct {
     uint64_t continued_solves;        /* site solves carried into a following step (a step gives every
                                          solving chain at most 8 Lanczos iterations) */
     uint64_t max_iterations_per_step; /* most Lanczos iterations one global step ran */
+    double seconds_replays;           /* with time_phases: device time of the Lanczos graph replays */
 } nc_batch_stats;
 typedef struct nc_batch nc_batch;
 

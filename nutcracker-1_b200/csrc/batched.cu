@@ -1266,8 +1266,12 @@ struct Engine {
     uint64_t global_steps = 0, lanczos_iterations = 0, graph_launches = 0, launches = 0;
     uint64_t continued_solves = 0, max_iterations_per_step = 0;
     double seconds = 0, seconds_moves = 0, seconds_solves = 0;   // the last two with time_phases
+    double seconds_replays = 0;   // device time of the Lanczos graph replays (time_phases)
+    cudaEvent_t ev_a = nullptr, ev_b = nullptr;
 
     ~Engine() {
+        if (ev_a) cudaEventDestroy(ev_a);
+        if (ev_b) cudaEventDestroy(ev_b);
         if (graph_exec) cudaGraphExecDestroy(graph_exec);
         if (graph) cudaGraphDestroy(graph);
         if (pool) cudaFree(pool);
@@ -1456,6 +1460,12 @@ struct Engine {
         grid_vec = sms * std::max(1, occ);
         NC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batched_qr_kernel, kQrThreads, 0));
         grid_qr = sms * std::max(1, occ);
+        // a small batch has fewer work items than a full persistent grid: launch
+        // no more CTAs than the largest work list can give work to
+        auto cap = [](int grid, size_t items) { return (int)std::max<size_t>(1, std::min<size_t>(grid, items)); };
+        grid_gemm = cap(grid_gemm, std::max(std::max(ntile_a, ntile_c), std::max(nmv1, nmv2)));
+        grid_mix = cap(grid_mix, nmix_items);
+        grid_vec = cap(grid_vec, nchunk_cap);
         NC_CUDA(cudaStreamSynchronize(stream));
     }
 
@@ -1799,6 +1809,13 @@ struct Engine {
         launches += 4;
         const int check_every = 4;
         uint64_t iters = 0;
+        if (opt.time_phases) {
+            if (!ev_a) {
+                NC_CUDA(cudaEventCreate(&ev_a));
+                NC_CUDA(cudaEventCreate(&ev_b));
+            }
+            NC_CUDA(cudaEventRecord(ev_a, stream));
+        }
         for (int it = 0; it < iteration_cap; ++it) {
             NC_CUDA(cudaGraphLaunch(graph_exec, stream));
             graph_launches++;
@@ -1808,6 +1825,13 @@ struct Engine {
             if ((it + 1) % check_every == 0 && read_active() == 0) break;
         }
         max_iterations_per_step = std::max(max_iterations_per_step, iters);
+        if (opt.time_phases) {
+            NC_CUDA(cudaEventRecord(ev_b, stream));
+            NC_CUDA(cudaEventSynchronize(ev_b));
+            float ms = 0;
+            NC_CUDA(cudaEventElapsedTime(&ms, ev_a, ev_b));
+            seconds_replays += ms * 1e-3;
+        }
         // the results of the solves that ended
         lz_form_kernel<2><<<grid_vec, kLzT, 0, stream>>>(lz_chunks.d.p, lz_chunks.d_count.p, d_lz.p, st, d_rz.p, d_solving.p,
                                                          d_part.p);
@@ -2067,6 +2091,7 @@ int nc_batch_get_stats(nc_batch* b, nc_batch_stats* st) {
     st->seconds = b->e.seconds;
     st->seconds_moves = b->e.seconds_moves;
     st->seconds_solves = b->e.seconds_solves;
+    st->seconds_replays = b->e.seconds_replays;
     st->continued_solves = b->e.continued_solves;
     st->max_iterations_per_step = b->e.max_iterations_per_step;
     st->device_bytes = b->e.pool_bytes;

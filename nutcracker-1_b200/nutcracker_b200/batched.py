@@ -56,6 +56,7 @@ class nc_batch_stats(ct.Structure):
         ("device_bytes", ct.c_uint64), ("seconds", ct.c_double),
         ("seconds_moves", ct.c_double), ("seconds_solves", ct.c_double),
         ("continued_solves", ct.c_uint64), ("max_iterations_per_step", ct.c_uint64),
+        ("seconds_replays", ct.c_double),
     ]
 
 
