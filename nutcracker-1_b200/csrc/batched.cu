@@ -44,6 +44,7 @@
 #include <memory>
 #include <vector>
 
+
 #include "batched_kernels.cuh"
 #include "nc_abi_util.h"
 #include "nc_common.cuh"
@@ -53,6 +54,7 @@
 namespace nc {
 namespace batch {
 namespace {
+
 
 // ---------------------------------------------------------------------------
 // Per-chain Lanczos state (read by every stage: a finished chain is skipped)
@@ -257,16 +259,15 @@ __device__ __forceinline__ void gemm_dispatch(const GProb& P, const cplx* A, int
 
 // Persistent: block b takes tiles b, b + grid, ...; tile t belongs to
 // problem tile_prob[t] and is its (t - prefix[problem])-th tile.
-__global__ void __launch_bounds__(kGemmThreads, 2) grouped_gemm_kernel(const GProb* __restrict__ probs,
-                                                                    const int* __restrict__ prefix,
-                                                                    const int* __restrict__ tile_prob,
-                                                                    const int* __restrict__ ntiles,
-                                                                    const LzState* __restrict__ st) {
-    extern __shared__ __align__(16) unsigned char smem[];
+// (The stage bodies below take the block's index vb among nvb blocks; each
+// kernel runs one of them over its whole grid.)
+__device__ __forceinline__ void gemm_phase(const GProb* __restrict__ probs, const int* __restrict__ prefix,
+                                           const int* __restrict__ tile_prob, const int* __restrict__ ntiles,
+                                           const LzState* __restrict__ st, unsigned char* smem, int vb, int nvb) {
     __shared__ GProb P;
     __shared__ int s_local;
     const int total = *ntiles;
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+    for (int t = vb; t < total; t += nvb) {
         __syncthreads();
         if (threadIdx.x == 0) {
             const int p = tile_prob[t];
@@ -283,19 +284,27 @@ __global__ void __launch_bounds__(kGemmThreads, 2) grouped_gemm_kernel(const GPr
     }
 }
 
+__global__ void __launch_bounds__(kGemmThreads, 2) grouped_gemm_kernel(const GProb* __restrict__ probs,
+                                                                    const int* __restrict__ prefix,
+                                                                    const int* __restrict__ tile_prob,
+                                                                    const int* __restrict__ ntiles,
+                                                                    const LzState* __restrict__ st) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    gemm_phase(probs, prefix, tile_prob, ntiles, st, smem, blockIdx.x, gridDim.x);
+}
+
 // ---------------------------------------------------------------------------
 // Grouped sparse-MPO mix (FP64 accumulation)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) grouped_mix_kernel(const MixProb* __restrict__ probs,
-                                                          const int2* __restrict__ items,
-                                                          const int* __restrict__ nitems,
-                                                          const LzState* __restrict__ st) {
+__device__ __forceinline__ void mix_phase(const MixProb* __restrict__ probs, const int2* __restrict__ items,
+                                          const int* __restrict__ nitems, const LzState* __restrict__ st, int vb,
+                                          int nvb) {
     __shared__ cplx Ws[kMixMaxNnz * kMixMaxD * kMixMaxD];
     __shared__ int k1s[kMixMaxNnz], k2s[kMixMaxNnz];
     __shared__ MixProb P;
     __shared__ int s_item;
     const int total = *nitems;
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+    for (int t = vb; t < total; t += nvb) {
         __syncthreads();
         if (threadIdx.x == 0) {
             const int2 it = items[t];
@@ -360,6 +369,13 @@ __global__ void __launch_bounds__(256) grouped_mix_kernel(const MixProb* __restr
     }
 }
 
+__global__ void __launch_bounds__(256) grouped_mix_kernel(const MixProb* __restrict__ probs,
+                                                          const int2* __restrict__ items,
+                                                          const int* __restrict__ nitems,
+                                                          const LzState* __restrict__ st) {
+    mix_phase(probs, items, nitems, st, blockIdx.x, gridDim.x);
+}
+
 // ---------------------------------------------------------------------------
 // Lanczos over every chain (FP64 basis, CGS2 reorthogonalisation)
 // ---------------------------------------------------------------------------
@@ -404,13 +420,13 @@ __device__ __forceinline__ void block_sum_c(double (&ar)[NK], double (&ai)[NK], 
 // the chunk.
 constexpr int kEpt = kVecChunk / kLzT;
 template <int PASS>
-__global__ void __launch_bounds__(kLzT) lz_cgs_kernel(const VChunk* __restrict__ chunks, const int* __restrict__ nchunks,
-                                                      const LzChain* __restrict__ ch, LzState* __restrict__ st,
-                                                      cplx* __restrict__ part) {
+__device__ __forceinline__ void cgs_phase(const VChunk* __restrict__ chunks, const int* __restrict__ nchunks,
+                                          const LzChain* __restrict__ ch, LzState* __restrict__ st,
+                                          cplx* __restrict__ part, int vb, int nvb) {
     __shared__ cplx red[kLzW * (kMaxKrylov + 1)];
     __shared__ cplx hs[kMaxKrylov + 1];
     const int total = *nchunks;
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+    for (int t = vb; t < total; t += nvb) {
         const VChunk c = chunks[t];
         const LzState& S = st[c.chain];
         if (S.done || S.stall) continue;
@@ -474,12 +490,17 @@ __global__ void __launch_bounds__(kLzT) lz_cgs_kernel(const VChunk* __restrict__
     }
 }
 
+template <int PASS>
+__global__ void __launch_bounds__(kLzT) lz_cgs_kernel(const VChunk* __restrict__ chunks, const int* __restrict__ nchunks,
+                                                      const LzChain* __restrict__ ch, LzState* __restrict__ st,
+                                                      cplx* __restrict__ part) {
+    cgs_phase<PASS>(chunks, nchunks, ch, st, part, blockIdx.x, gridDim.x);
+}
+
 // Per chain (one warp): h = sum of the chain's chunk partials in chunk order.
 template <int PASS>
-__global__ void lz_reduce_kernel(int nchains, const LzChain* __restrict__ ch, LzState* __restrict__ st,
-                                 const cplx* __restrict__ part) {
-    const int c = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32, lane = threadIdx.x & 31;
-    if (c >= nchains) return;
+__device__ __forceinline__ void reduce_chain(int c, int lane, const LzChain* __restrict__ ch, LzState* __restrict__ st,
+                                             const cplx* __restrict__ part) {
     LzState& S = st[c];
     if (S.done || S.stall) return;
     const int nk = (PASS < 2) ? S.j + 1 : 1;
@@ -496,18 +517,20 @@ __global__ void lz_reduce_kernel(int nchains, const LzChain* __restrict__ ch, Lz
     else S.wn2 = x;
 }
 
+template <int PASS>
+__global__ void lz_reduce_kernel(int nchains, const LzChain* __restrict__ ch, LzState* __restrict__ st,
+                                 const cplx* __restrict__ part) {
+    const int c = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32, lane = threadIdx.x & 31;
+    if (c < nchains) reduce_chain<PASS>(c, lane, ch, st, part);
+}
+
 // One warp per chain: column j of the projected matrix from the
 // reorthogonalisation coefficients, the Ritz pairs (warm-started Jacobi,
 // nc_ritz.cuh), and the decision: converged (ARPACK's rule, Ritz estimate
 // <= tol * max(|theta|, eps^(2/3)), or the Krylov space exhausted or
 // invariant), basis full (thick restart), or advance.
-__global__ void __launch_bounds__(32) lz_ritz_kernel(int nchains, const LzChain* __restrict__ ch,
-                                                     LzState* __restrict__ st, LzRitz* __restrict__ rz,
-                                                     int* __restrict__ active) {
-    __shared__ RitzSmem<kMaxKrylov> w;
-    const int c = blockIdx.x;
-    if (c == 0 && threadIdx.x == 0) *active = 0;
-    if (c >= nchains) return;
+__device__ __forceinline__ void ritz_chain(int c, RitzSmem<kMaxKrylov>& w, const LzChain* __restrict__ ch,
+                                           LzState* __restrict__ st, LzRitz* __restrict__ rz) {
     LzState& S = st[c];
     if (S.done || S.stall) return;
     const LzChain C = ch[c];
@@ -516,7 +539,7 @@ __global__ void __launch_bounds__(32) lz_ritz_kernel(int nchains, const LzChain*
     const RitzResult r =
         ritz_update_warp<kMaxKrylov, false>(w, j + 1, R.state, S.h1, S.h2, fmax(S.wn2, 0.0), RITZ_SR, R.S,
                                             kMaxKrylov, R.theta);
-    if (threadIdx.x != 0) return;
+    if ((threadIdx.x & 31) != 0) return;
     S.matvecs++;
     S.theta = r.theta;
     S.res = r.res;
@@ -534,11 +557,20 @@ __global__ void __launch_bounds__(32) lz_ritz_kernel(int nchains, const LzChain*
     }
 }
 
+__global__ void __launch_bounds__(32) lz_ritz_kernel(int nchains, const LzChain* __restrict__ ch,
+                                                     LzState* __restrict__ st, LzRitz* __restrict__ rz,
+                                                     int* __restrict__ active) {
+    __shared__ RitzSmem<kMaxKrylov> w;
+    const int c = blockIdx.x;
+    if (c == 0 && threadIdx.x == 0) *active = 0;
+    if (c < nchains) ritz_chain(c, w, ch, st, rz);
+}
+
 // V_{j+1} = w / beta_j for the chains that advance.
-__global__ void __launch_bounds__(kLzT) lz_next_kernel(const VChunk* __restrict__ chunks, const int* __restrict__ nchunks,
-                                                       const LzChain* __restrict__ ch, const LzState* __restrict__ st) {
+__device__ __forceinline__ void next_phase(const VChunk* __restrict__ chunks, const int* __restrict__ nchunks,
+                                                       const LzChain* __restrict__ ch, const LzState* __restrict__ st, int vb, int nvb) {
     const int total = *nchunks;
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+    for (int t = vb; t < total; t += nvb) {
         const VChunk c = chunks[t];
         const LzState& S = st[c.chain];
         if (!S.adv) continue;
@@ -547,6 +579,11 @@ __global__ void __launch_bounds__(kLzT) lz_next_kernel(const VChunk* __restrict_
         cplx* vn = C.V + (long long)(S.j + 1) * C.n;
         for (int i = c.off + threadIdx.x; i < c.off + c.len; i += kLzT) vn[i] = cscale(C.w[i], f);
     }
+}
+
+__global__ void __launch_bounds__(kLzT) lz_next_kernel(const VChunk* __restrict__ chunks, const int* __restrict__ nchunks,
+                                                       const LzChain* __restrict__ ch, const LzState* __restrict__ st) {
+    next_phase(chunks, nchunks, ch, st, blockIdx.x, gridDim.x);
 }
 
 __global__ void lz_inc_kernel(int nchains, LzState* __restrict__ st, int* __restrict__ active) {
@@ -693,14 +730,14 @@ __global__ void __launch_bounds__(kLzT) lz_scale_kernel(const VChunk* __restrict
 // ---- thick restart (Wu & Simon 2000), for the chains whose basis is full ---
 // Y_i = V S(:,i) for the `keep` wanted Ritz vectors, Y_keep = w / beta (the
 // residual direction, orthogonal to them).
-__global__ void __launch_bounds__(kLzT) lz_restart_form_kernel(const VChunk* __restrict__ chunks,
+__device__ __forceinline__ void restart_form_phase(const VChunk* __restrict__ chunks,
                                                                const int* __restrict__ nchunks,
                                                                const LzChain* __restrict__ ch,
                                                                const LzState* __restrict__ st,
-                                                               const LzRitz* __restrict__ rz) {
+                                                               const LzRitz* __restrict__ rz, int vb, int nvb) {
     __shared__ double ss[kKeepMax * kMaxKrylov];
     const int total = *nchunks;
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+    for (int t = vb; t < total; t += nvb) {
         const VChunk c = chunks[t];
         const LzState& S = st[c.chain];
         if (S.done || !S.stall) continue;
@@ -726,13 +763,21 @@ __global__ void __launch_bounds__(kLzT) lz_restart_form_kernel(const VChunk* __r
     }
 }
 
-// V_0..V_keep = Y_0..Y_keep.
-__global__ void __launch_bounds__(kLzT) lz_restart_copy_kernel(const VChunk* __restrict__ chunks,
+__global__ void __launch_bounds__(kLzT) lz_restart_form_kernel(const VChunk* __restrict__ chunks,
                                                                const int* __restrict__ nchunks,
                                                                const LzChain* __restrict__ ch,
-                                                               const LzState* __restrict__ st) {
+                                                               const LzState* __restrict__ st,
+                                                               const LzRitz* __restrict__ rz) {
+    restart_form_phase(chunks, nchunks, ch, st, rz, blockIdx.x, gridDim.x);
+}
+
+// V_0..V_keep = Y_0..Y_keep.
+__device__ __forceinline__ void restart_copy_phase(const VChunk* __restrict__ chunks,
+                                                               const int* __restrict__ nchunks,
+                                                               const LzChain* __restrict__ ch,
+                                                               const LzState* __restrict__ st, int vb, int nvb) {
     const int total = *nchunks;
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+    for (int t = vb; t < total; t += nvb) {
         const VChunk c = chunks[t];
         const LzState& S = st[c.chain];
         if (S.done || !S.stall) continue;
@@ -741,6 +786,13 @@ __global__ void __launch_bounds__(kLzT) lz_restart_copy_kernel(const VChunk* __r
             for (int i = c.off + threadIdx.x; i < c.off + c.len; i += kLzT)
                 C.V[(long long)q * C.n + i] = C.Y[(long long)q * C.n + i];
     }
+}
+
+__global__ void __launch_bounds__(kLzT) lz_restart_copy_kernel(const VChunk* __restrict__ chunks,
+                                                               const int* __restrict__ nchunks,
+                                                               const LzChain* __restrict__ ch,
+                                                               const LzState* __restrict__ st) {
+    restart_copy_phase(chunks, nchunks, ch, st, blockIdx.x, gridDim.x);
 }
 
 // Per chain (one block): the projected matrix becomes diag(theta_0 ..
@@ -1466,6 +1518,7 @@ struct Engine {
         grid_gemm = cap(grid_gemm, std::max(std::max(ntile_a, ntile_c), std::max(nmv1, nmv2)));
         grid_mix = cap(grid_mix, nmix_items);
         grid_vec = cap(grid_vec, nchunk_cap);
+
         NC_CUDA(cudaStreamSynchronize(stream));
     }
 
