@@ -7,7 +7,8 @@ so the cases can run side by side):
     python tests/golden/make_scale_fixtures.py --merge
 
 Each run writes ``tests/golden/scale/<case>.json``; ``--merge`` combines them
-into ``tests/golden/scale_levels.json``, which the ``-m gpu`` tests read.
+into ``tests/golden/scale_levels.json``, which the ``-m gpu`` tests read, and
+records a fingerprint of every case's initial states beside its results.
 One BLAS thread per process: the site problems are small (n = chi^2 d =
 8192 at chi=64), and a multi-threaded BLAS spends its time spinning.
 """
@@ -31,6 +32,9 @@ def main():
         for p in sorted(glob.glob(os.path.join(out_dir, "*.json"))):
             with open(p) as f:
                 d = json.load(f)
+            # pins the initial states that the GPU tests replay to the ones the
+            # oracle started from
+            d["initial_states_fingerprint"] = scale_cases.fingerprint(scale_cases.initial_states(d["case"]))
             merged[d["case"]] = d
         with open(os.path.join(HERE, "scale_levels.json"), "w") as f:
             json.dump(merged, f, indent=1)

@@ -17,12 +17,15 @@ level can be replayed without solving anything (``initial_states``).
 from __future__ import annotations
 
 import numpy as np
+from threadpoolctl import threadpool_limits
 
 from oracle import driver, mpo
 
 # name -> (operator builder, sites, chi, levels, seed)
 CASES = {
-    "heisenberg_xxx_N100_chi64": (lambda n: mpo.heisenberg(n), 100, 64, 3, 2024),
+    "heisenberg_xxx_N100_chi64": (lambda n: mpo.heisenberg(n), 100, 64, 1, 2024),
+    "heisenberg_xxx_N100_chi128": (lambda n: mpo.heisenberg(n), 100, 128, 1, 2026),
+    "tfim_lambda1.5_N100_chi32": (lambda n: mpo.transverse_ising_ferro(n, 1.5), 100, 32, 3, 2027),
     "spin1_heisenberg_D0.5_N64_chi64": (lambda n: mpo.heisenberg_spin1(n, 0.5), 64, 64, 1, 2025),
 }
 ARPACK_NCV = 24
@@ -40,8 +43,41 @@ def options(name, **kw):
 
 def initial_states(name):
     """The initial state of every level, as the oracle's level loop draws them."""
-    _, _, _, levels, seed = CASES[name]
-    ch = driver.Chain(operator(name), options(name), seed=seed)
+    _, _, chi, levels, seed = CASES[name]
+    return draw_initial_states(operator(name), chi, levels, seed)
+
+
+def draw_initial_states(ops, chi, levels, seed):
+    """The sites that ``levels`` resets of ``driver.Chain(ops, seed=seed)`` at
+    bond dimension ``chi`` draw from their ``InitialSiteSource``, without
+    contracting any environment: each reset (chain.cpp:175-237) draws the
+    right-normalised sites N-1 .. 1, then the centre site 0.  The projectors
+    that the level loop adds in between draw nothing, and at these bond
+    dimensions they do not raise the chain's bond dimension
+    (minimum_bandwidth_dimension_for_projector_count), so the draws are the
+    same.  ``replay_initial_states`` is the reference for this shortcut."""
+    with threadpool_limits(1):   # small QRs: a threaded BLAS only spins
+        return _draw(ops, chi, levels, seed)
+
+
+def _draw(ops, chi, levels, seed):
+    phys = [o.d for o in ops]
+    n = len(ops)
+    bw = min(driver.maximum_bandwidth_dimension(phys), chi)
+    dims = driver.compute_bandwidth_dimension_sequence(bw, phys)
+    rdims = list(reversed(dims))
+    src = driver.InitialSiteSource(seed)
+    out = []
+    for _ in range(levels):
+        rights = [src.right(ops[op].d, rdims[k + 1], rdims[k]) for k, op in enumerate(reversed(range(1, n)))]
+        centre = src.middle(ops[0].d, dims[0], dims[1])
+        out.append([np.asfortranarray(centre)] + [np.asfortranarray(s) for s in reversed(rights)])
+    return out
+
+
+def replay_initial_states(ops, chi, levels, seed):
+    """The same states read from the oracle's own chain after each reset."""
+    ch = driver.Chain(ops, driver.ChainOptions(initial_bandwidth_dimension=chi), seed=seed)
     out = [[s.copy(order="F") for s in ch.state_sites()]]
     for _ in range(1, levels):
         ch.reset()
@@ -49,9 +85,29 @@ def initial_states(name):
     return out
 
 
+def fingerprint(states):
+    """Per level, two weighted sums over every site's elements (real and
+    imaginary part): enough to show a change of seed or draw order, and
+    insensitive to the last-bit differences that another BLAS build or
+    thread count leaves in the QRs of the random sites."""
+    out = []
+    for level in states:
+        acc = 0j
+        for i, s in enumerate(level):
+            a = np.asarray(s).ravel(order="F")
+            acc += (i + 1) * np.dot(np.arange(1, a.size + 1) % 7 + 1, a)
+        out.append([float(acc.real), float(acc.imag)])
+    return out
+
+
 def entanglement_profile(sites):
     """Von Neumann entropy of the normalised state across every bond (a
     gauge-invariant fingerprint of an MPS); sites (br, bl, d), any gauge."""
+    with threadpool_limits(1):
+        return _entanglement_profile(sites)
+
+
+def _entanglement_profile(sites):
     n = len(sites)
     # left-canonicalise from site 0, reading the Schmidt values of each bond
     # from the singular values of the remainder carried to the right
