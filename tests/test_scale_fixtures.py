@@ -50,3 +50,22 @@ def test_fixtures_match_the_case_table():
         assert all(a <= b + 1e-9 * abs(b) for a, b in zip(fx["energies"], fx["energies"][1:]))
         np.testing.assert_allclose(scale_cases.fingerprint(scale_cases.initial_states(name)),
                                    fx["initial_states_fingerprint"], rtol=1e-9)
+
+
+def test_tfim_fixture_is_exact():
+    """The oracle's three N=100 transverse Ising levels (projector method,
+    chi=32) against the exact free-fermion levels: the fixture that the GPU
+    is compared with is itself pinned to an exact answer at scale."""
+    with open(os.path.join(HERE, "golden", "scale_levels.json")) as f:
+        fx = json.load(f)["tfim_lambda1.5_N100_chi32"]
+    n, lam = fx["sites"], 1.5
+    A = np.diag(np.full(n, 2.0 * lam))
+    B = np.zeros((n, n))
+    for i in range(n - 1):
+        A[i, i + 1] = A[i + 1, i] = -1.0
+        B[i, i + 1], B[i + 1, i] = -1.0, 1.0
+    L = np.sort(np.abs(np.linalg.eigvalsh(np.block([[A, B], [-B, -A]]))[n:]))
+    e0 = -0.5 * float(L.sum())
+    exact = [e0, e0 + L[0], e0 + L[1]]
+    for got, want in zip(fx["energies"], exact):
+        assert abs(got - want) / n <= 1e-13, (fx["energies"], exact)
