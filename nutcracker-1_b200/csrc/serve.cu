@@ -125,6 +125,11 @@ void nc_server::worker() {
             }
             nc_chain_free(ch);
         }
+        // the request's copy of its operator is not needed once its chain is
+        // gone; only the (small) result stays with the request id
+        std::vector<std::vector<uint32_t>>().swap(r->idx);
+        std::vector<std::vector<nc_complex>>().swap(r->W);
+        std::vector<nc_operator_site>().swap(r->sites);
         {
             std::lock_guard<std::mutex> lk(mu);
             r->t_done = Clock::now();
