@@ -148,9 +148,24 @@ class Parser {
   private:
     std::vector<Line> lines_;
     std::map<std::string, YPtr> anchors_;
+    // Nesting depth of the recursive descent; operator files nest a few
+    // levels, and a bound keeps malformed input from exhausting the stack.
+    static constexpr int kMaxDepth = 256;
+    int depth_ = 0;
+    struct Nest {
+        int& d;
+        Nest(int& depth, int number) : d(depth) {
+            if (d >= kMaxDepth)
+                fail("YAML: nesting deeper than " + std::to_string(kMaxDepth) + " levels on line " +
+                     std::to_string(number));
+            ++d;
+        }
+        ~Nest() { --d; }
+    };
 
     YPtr block(size_t& i, int indent) {
         const Line& l = lines_[i];
+        Nest nest(depth_, l.number);
         if (is_seq_item(l.text)) return sequence(i, l.indent);
         if (key_separator(l.text) != std::string::npos && l.text[0] != '[' && l.text[0] != '{')
             return mapping(i, l.indent);
@@ -284,6 +299,7 @@ class Parser {
     }
 
     YPtr flow(const std::string& s, size_t& p, int number) {
+        Nest nest(depth_, number);
         skip_ws(s, p);
         if (p < s.size() && s[p] == '&') {
             size_t e = p + 1;
@@ -427,6 +443,9 @@ UniqueSite read_site(const YNode& node) {
     const long long cl = as_integer(node.get("left dimension"), "left dimension");
     const long long cr = as_integer(node.get("right dimension"), "right dimension");
     if (d < 1 || cl < 1 || cr < 1) fail("YAML: site dimensions must be positive");
+    // the dimensions are unsigned 32-bit integers in the operator format
+    if (d > UINT32_MAX || cl > UINT32_MAX || cr > UINT32_MAX)
+        fail("YAML: site dimensions must be below 2^32");
     s.d = (uint32_t)d;
     s.cl = (uint32_t)cl;
     s.cr = (uint32_t)cr;

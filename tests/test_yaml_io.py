@@ -165,6 +165,24 @@ def test_malformed_yaml_is_rejected(yio):
             yio.read_operator(bad)
 
 
+def test_hostile_input_fails_with_a_message(yio):
+    """Deep nesting is bounded (the parser recurses per level) and dimensions
+    past the format's unsigned 32-bit range are rejected before any size
+    computed from them is used."""
+    from nutcracker_b200 import NutcrackerError
+    for deep in ["[" * 100000, "- " * 100000 + "1", "a: " + "[" * 300 + "]" * 300 + "\n"]:
+        with pytest.raises(NutcrackerError, match="nesting deeper than 256 levels"):
+            yio.read_operator(deep)
+    shallow = "sites: " + "[" * 200 + "]" * 200 + "\n"
+    with pytest.raises(NutcrackerError, match="'sites' must be a list|every entry"):
+        yio.read_operator(shallow)
+    site = ("  - physical dimension: {d}\n    left dimension: 1\n    right dimension: 1\n    matrices:\n"
+            "      - from: 1\n        to: 1\n        data: [1,0,0,1]\n")
+    for d in (4294967296, 99999999999):
+        with pytest.raises(NutcrackerError, match="below 2\\^32"):
+            yio.read_operator("sequence: [1]\nsites:\n" + site.format(d=d))
+
+
 def test_line_endings_quoted_keys_and_flow_documents(yio):
     text = open(os.path.join(HERE, "golden", "yaml", "external_field_anchors_5.yaml")).read()
     want = yio.read_operator(text)
