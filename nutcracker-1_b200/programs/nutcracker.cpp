@@ -24,6 +24,7 @@
 // B200 additions: --precision 1 (3xTF32 tensor-core sweeps closed by FP64
 // refinement), --seed, --initial-bandwidth (first chi of optimizeChain's
 // growth schedule).
+#include <cerrno>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -172,11 +173,14 @@ double to_double(const Values& v, const char* name) {
     return x;
 }
 
-unsigned long long to_unsigned(const Values& v, const char* name) {
+// An unsigned option value no larger than `max` (the 32-bit options of the
+// reference by default); anything else is invalid, as a failed conversion is.
+unsigned long long to_unsigned(const Values& v, const char* name, unsigned long long max = UINT32_MAX) {
     const std::string& s = v.at(name);
     char* end = nullptr;
+    errno = 0;
     const unsigned long long x = std::strtoull(s.c_str(), &end, 10);
-    if (end == s.c_str() || *end || s[0] == '-')
+    if (end == s.c_str() || *end || s[0] == '-' || errno == ERANGE || x > max)
         throw OptionError(std::string("the argument ('") + s + "') for option '--" + name + "' is invalid");
     return x;
 }
@@ -318,7 +322,7 @@ int run(const Values& v) {
     if (v.count("chain-tolerance")) o.chain_convergence_threshold = to_double(v, "chain-tolerance");
     if (v.count("sanity-tolerance")) o.sanity_check_threshold = to_double(v, "sanity-tolerance");
     if (v.count("precision")) o.precision = (uint32_t)to_unsigned(v, "precision");
-    if (v.count("seed")) o.seed = to_unsigned(v, "seed");
+    if (v.count("seed")) o.seed = to_unsigned(v, "seed", UINT64_MAX);
     if (v.count("initial-bandwidth")) o.initial_bandwidth_dimension = (uint32_t)to_unsigned(v, "initial-bandwidth");
     const std::string mode = v.count("optimizer-mode") ? v.at("optimizer-mode") : std::string("<v");
     std::snprintf(o.optimizer_mode, sizeof o.optimizer_mode, "%s", mode.c_str());

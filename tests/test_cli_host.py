@@ -32,6 +32,10 @@ def test_help_listings_exit_1():
     (["--no-such-option"], b"unrecognised option '--no-such-option'"),
     (["-n"], b"the required argument for option '--number-of-levels' is missing"),
     (["--site-tolerance", "abc"], b"the argument ('abc') for option '--site-tolerance' is invalid"),
+    # unsigned 32-bit options: values past the range fail as a conversion does
+    (["-n", "4294967296"], b"the argument ('4294967296') for option '--number-of-levels' is invalid"),
+    (["-n", "99999999999999999999"], b"the argument ('99999999999999999999') for option '--number-of-levels' is invalid"),
+    (["-n", "-1"], b"the argument ('-1') for option '--number-of-levels' is invalid"),
 ])
 def test_option_errors_exit_255(args, message):
     r = run(args)
